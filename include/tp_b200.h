@@ -1,0 +1,244 @@
+/*
+ * tp_b200.h - C ABI of the B200-native (sm_100a) tile processor.
+ *
+ * Drop-in host entry points for the frequency-domain tile processor of
+ * mfkiwl/tile_processor_gpu.  Each tp_* call replaces one `extern "C"
+ * __global__` kernel of the reference (launched there with <<<>>> by
+ * src/dtt8x8.cu or by name through JCuda) and takes the same arguments, in the
+ * same order and with the same meaning, plus:
+ *   - a tp_geometry block that replaces the reference's compile-time
+ *     IMG_WIDTH / IMG_HEIGHT / KERNELS_* / TILES* defines
+ *     (src/TileProcessor.cuh:43-73,145-175), so one library serves every frame
+ *     size;
+ *   - the CUDA stream to launch on (NULL = legacy default stream).
+ *
+ * Buffers are caller-owned device memory, exactly as in the reference
+ * (src/dtt8x8.cu:53-142): pitched float images, per-camera pointer arrays that
+ * live in device memory (float ** on the device), pitched outputs.  Strides are
+ * in floats.  Outputs that the reference accumulates into (imclt_rbg, the RGBA
+ * texture image) are accumulated here too.
+ *
+ * Every call validates its host-visible arguments and returns TP_OK or a
+ * negative TP_ERR_* code (the reference kernels return void and silently skip
+ * bad input); tp_last_error() gives a one-line reason.  No call allocates
+ * device memory, synchronises the device or reads device data on the host.
+ * Device-side inputs that the host cannot see (task records, index lists) are
+ * range-checked in the kernels: an out-of-range entry is skipped instead of
+ * being read or written out of bounds.
+ */
+#ifndef TP_B200_H
+#define TP_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *tp_stream_t; /* same object as cudaStream_t */
+
+/* ---- fixed sizes (the reference hard-codes the same values) ---------------- */
+#define TP_DTT_SIZE        8   /* DTT_SIZE            src/dtt8x8.cuh:52        */
+#define TP_NUM_CAMS        4   /* NUM_CAMS            src/TileProcessor.cuh:44 */
+#define TP_NUM_PAIRS       6   /* NUM_PAIRS           src/TileProcessor.cuh:45 */
+#define TP_NUM_COLORS      3   /* NUM_COLORS          src/TileProcessor.cuh:46 */
+#define TP_CORR_NTILE_SHIFT 8  /* CORR_NTILE_SHIFT    src/TileProcessor.cuh:60 */
+#define TP_TASK_CORR_BITS  4   /* TASK_CORR_BITS      src/TileProcessor.cuh:63 */
+#define TP_LIST_TEXTURE_BIT 7  /* LIST_TEXTURE_BIT    src/TileProcessor.cuh:69 */
+#define TP_TASK_TEXTURE_BITS 0xf /* N/E/S/W bits 0..3 src/TileProcessor.cuh:64-67,96 */
+#define TP_MAX_CORR_RADIUS 7   /* (2r+1)^2 <= 15x15   src/TileProcessor.cuh:2950-3008 */
+
+/* Per-tile task record, byte-identical to `struct tp_task`
+ * (src/TileProcessor.cuh:179-186) with NUM_CAMS = 4: 40 bytes.
+ *   task : bits 0..3 texture N/E/S/W, bits 4..9 correlation pair mask;
+ *   txy  : tile x in bits 0..15, tile y in bits 16..31;
+ *   xy   : tile centre in each camera's pixel coordinates. */
+typedef struct tp_task {
+    int   task;
+    int   txy;
+    float xy[TP_NUM_CAMS][2];
+} tp_task;
+
+/* Kernel-tile offsets, byte-identical to `struct CltExtra`
+ * (src/TileProcessor.cuh:187-196): 8 floats per kernel tile. */
+typedef struct tp_clt_extra {
+    float data_x, data_y, center_x, center_y;
+    float dxc_dx, dxc_dy, dyc_dx, dyc_dy;
+} tp_clt_extra;
+
+/* How the Bayer fetch treats tiles whose 16x16 window leaves the image. */
+enum {
+    /* The reference's addressing (src/TileProcessor.cuh:3183-3193,3328-3361):
+     * right-edge corner clamp `itlx & 1 + (W-10)` (C precedence: itlx & (W-9)),
+     * columns clamped with IMG_HEIGHT/2 and rows with IMG_WIDTH/2.  Reads that
+     * the reference makes past the end of the caller's image allocation
+     * (tp_geometry.image_rows rows of dstride floats) read the allocation's last
+     * float instead; every other read is at the reference's address. */
+    TP_BORDER_REFERENCE = 0,
+    /* Same corner logic with the precedence fixed, and every pixel clamped
+     * into the image by Bayer pairs (columns to W, rows to H). */
+    TP_BORDER_CLAMP = 1
+};
+
+/* Runtime geometry (the reference's compile-time defines). */
+typedef struct tp_geometry {
+    int img_width;      /* IMG_WIDTH, multiple of 8, >= 32                     */
+    int img_height;     /* IMG_HEIGHT, multiple of 8, >= 32                    */
+    int kernels_hor;    /* KERNELS_HOR   (kernel-table columns)                */
+    int kernels_vert;   /* KERNELS_VERT  (kernel-table rows)                   */
+    int kernels_lstep;  /* KERNELS_LSTEP (kernel grid step = 1 << lstep px)    */
+    int image_rows;     /* rows allocated per source image, >= img_height      */
+    int border_mode;    /* TP_BORDER_REFERENCE or TP_BORDER_CLAMP              */
+    int debug_marks;    /* 1: imclt_rbg also makes the reference's debug writes
+                           (tile (0,0) := 100, tile (161,111) doubled,
+                           src/TileProcessor.cuh:2687-2700); 0: plain output */
+} tp_geometry;
+
+/* Status codes. */
+enum {
+    TP_OK            = 0,
+    TP_ERR_ARG       = -1, /* NULL pointer, negative count, bad stride/radius  */
+    TP_ERR_GEOMETRY  = -2, /* inconsistent tp_geometry                         */
+    TP_ERR_CUDA      = -3, /* a CUDA runtime call or launch failed             */
+    TP_ERR_UNSUPPORTED = -4, /* valid in the reference, not in this build      */
+    TP_ERR_NO_DEVICE = -5  /* no CUDA device visible                           */
+};
+
+/* One-line description of the last error on the calling thread. */
+const char *tp_last_error(void);
+/* Library version string. */
+const char *tp_version(void);
+
+/* Tiles per row / column (TILESX, TILESY, TILESYA of src/TileProcessor.cuh:146-149). */
+int tp_tiles_x(const tp_geometry *g);
+int tp_tiles_y(const tp_geometry *g);
+int tp_tiles_ya(const tp_geometry *g);
+
+/* ---- constant tables --------------------------------------------------------
+ * The reference keeps its low-pass filters in __constant__ memory and lets the
+ * caller overwrite them with cudaMemcpyToSymbol (src/TileProcessor.cuh:421-481).
+ * which: 0..3 = lpf_data[0..3] (R, B, G, mono), 4 = lpf_rb_corr, 5 = lpf_corr.
+ * values: 64 floats, row-major 8x8.  Applies to the current CUDA device. */
+int tp_set_lpf(int which, const float *values);
+int tp_get_lpf(int which, float *values);
+/* Restore the built-in tables on the current device. */
+int tp_reset_lpf(void);
+
+/* ---- forward CLT with aberration correction ---------------------------------
+ * Replaces convert_correct_tiles (src/TileProcessor.cuh:1859-1937).
+ * kernel_offsets : device array [4] of device tp_clt_extra[kv*kh*3]
+ * kernels        : device array [4] of device float[kv*kh*3*4*64]
+ * images         : device array [4] of device float[image_rows][dstride]
+ * tasks          : device tp_task[num_tiles]; tasks with task == 0 are skipped
+ * clt            : device array [4] of device float[tilesy*tilesx*3*4*64]
+ * lpf_mask       : bit c applies lpf_data[c] to color c */
+int tp_convert_correct_tiles(const tp_geometry *g,
+                             float *const *kernel_offsets,
+                             float *const *kernels,
+                             float *const *images,
+                             const tp_task *tasks,
+                             float *const *clt,
+                             size_t dstride,
+                             int num_tiles,
+                             int lpf_mask,
+                             tp_stream_t stream);
+
+/* ---- pairwise phase correlation ---------------------------------------------
+ * Replaces correlate2D (src/TileProcessor.cuh:1176-1443).
+ * corr_indices : device int[num_corr_tiles], (tile << 8) | pair, pair 0..5
+ * corrs        : device float, tile i's (2r+1)^2 floats at corrs + i*corr_stride */
+int tp_correlate2D(const tp_geometry *g,
+                   float *const *clt,
+                   int colors,
+                   float scale0, float scale1, float scale2,
+                   float fat_zero,
+                   size_t num_corr_tiles,
+                   const int *corr_indices,
+                   size_t corr_stride,
+                   int corr_radius,
+                   float *corrs,
+                   tp_stream_t stream);
+
+/* ---- texture tiles -----------------------------------------------------------
+ * Replaces textures_accumulate (src/TileProcessor.cuh:2207-2579).
+ * texture_indices : device int[num_texture_tiles], (tile << 8) | (1 << 7) | nbr
+ * woi             : device int[4] {x, y, width, height} in tiles (read only
+ *                   when texture_rbg is used)
+ * port_offsets    : device float[4][2]
+ * texture_rbg     : overlapped RGBA image, += (NULL or stride 0 = skip)
+ * texture_tiles   : non-overlapped 16x16 tiles, tile i at i*texture_stride
+ *                   (NULL or stride 0 = skip) */
+int tp_textures_accumulate(const tp_geometry *g,
+                           const int *woi,
+                           float *const *clt,
+                           size_t num_texture_tiles,
+                           const int *texture_indices,
+                           const float *port_offsets,
+                           int colors, int is_lwir,
+                           float min_shot, float scale_shot,
+                           float diff_sigma, float diff_threshold,
+                           float min_agree,
+                           float weight0, float weight1, float weight2,
+                           int dust_remove, int keep_weights,
+                           size_t texture_rbg_stride, float *texture_rbg,
+                           size_t texture_stride, float *texture_tiles,
+                           tp_stream_t stream);
+
+/* ---- inverse CLT into an image -----------------------------------------------
+ * Replaces imclt_rbg (src/TileProcessor.cuh:2588-2710): one of the 4 parity
+ * passes of one color plane.  rbg: device float[3*(H+8)][dstride], dstride >=
+ * W + 8.  Pass (0,0) overwrites, the others accumulate. */
+int tp_imclt_rbg(const tp_geometry *g,
+                 const float *clt_one_cam,
+                 float *rbg,
+                 int color, int v_offset, int h_offset,
+                 size_t dstride,
+                 tp_stream_t stream);
+/* All 3 colors x 4 passes of one camera in the order the reference's driver
+ * issues them (src/dtt8x8.cu:624-662), in one call. */
+int tp_imclt_rbg_all(const tp_geometry *g,
+                     const float *clt_one_cam,
+                     float *rbg,
+                     size_t dstride,
+                     tp_stream_t stream);
+
+/* ---- texture list and RGBA driver --------------------------------------------
+ * Replace the dynamic-parallelism drivers prepare_texture_list
+ * (src/TileProcessor.cuh:1643-1713) and generate_RBGA (:1446-1615) with
+ * host-launched kernels on one stream (no device-side launches, no host sync).
+ * texture_indices   : device int[tilesx * tilesya]
+ * num_texture_tiles : device int[8] (inner/border count per 2x2 parity)
+ * woi               : device int[4] -> {x, y, width, height} in tiles
+ * Lists are in task order (the reference's order depends on atomicAdd order).
+ * tasks' bits 0..3 are rewritten with the N/E/S/W neighbour mask, as in the
+ * reference. */
+int tp_prepare_texture_list(const tp_geometry *g,
+                            tp_task *tasks, int num_tiles,
+                            int *texture_indices, int *num_texture_tiles,
+                            int *woi, int width, int height,
+                            tp_stream_t stream);
+
+int tp_clear_texture_rbga(const tp_geometry *g,
+                          int texture_width, int texture_slice_height,
+                          size_t texture_rbga_stride, float *texture_tiles,
+                          tp_stream_t stream);
+
+int tp_generate_RBGA(const tp_geometry *g,
+                     tp_task *tasks, int num_tiles,
+                     int *texture_indices, int *num_texture_tiles,
+                     int *woi, int width, int height,
+                     float *const *clt,
+                     const float *port_offsets,
+                     int colors, int is_lwir,
+                     float min_shot, float scale_shot,
+                     float diff_sigma, float diff_threshold,
+                     float min_agree,
+                     float weight0, float weight1, float weight2,
+                     int dust_remove, int keep_weights,
+                     size_t texture_rbga_stride, float *texture_tiles,
+                     tp_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TP_B200_H */

@@ -1,0 +1,348 @@
+/*
+ * tp_api.cu - C ABI of the B200 tile processor (declared in include/tp_b200.h).
+ *
+ * Each entry point checks its host-visible arguments, converts the geometry,
+ * sizes the grid from the device's SM count and launches on the caller's
+ * stream.  Nothing here allocates, synchronises or copies device data to the
+ * host.
+ */
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "tp_common.cuh"
+#include "tp_convert.cuh"
+#include "tp_correlate.cuh"
+#include "tp_texture.cuh"
+#include "tp_imclt.cuh"
+#include "tp_list.cuh"
+
+#define TP_VERSION "tile_processor_gpu_b200 0.1 (sm_100a)"
+
+namespace {
+
+thread_local char g_err[512] = "no error";
+
+int fail(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_status(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) return fail(TP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return TP_OK;
+}
+
+int check_geometry(const tp_geometry *g, tp::Geom *out)
+{
+    if (!g) return fail(TP_ERR_ARG, "geometry is NULL");
+    if (g->img_width < 32 || g->img_height < 32 || (g->img_width & 7) || (g->img_height & 7))
+        return fail(TP_ERR_GEOMETRY, "image %dx%d: width and height must be multiples of 8, >= 32",
+                    g->img_width, g->img_height);
+    if (g->img_width > (1 << 15) || g->img_height > (1 << 15))
+        return fail(TP_ERR_GEOMETRY, "image %dx%d exceeds 32768", g->img_width, g->img_height);
+    if (g->kernels_lstep < 1 || g->kernels_lstep > 8)
+        return fail(TP_ERR_GEOMETRY, "kernels_lstep %d outside 1..8", g->kernels_lstep);
+    if (g->kernels_hor < 1 || g->kernels_vert < 1)
+        return fail(TP_ERR_GEOMETRY, "kernel grid %dx%d", g->kernels_hor, g->kernels_vert);
+    if (g->image_rows < g->img_height)
+        return fail(TP_ERR_GEOMETRY, "image_rows %d < img_height %d", g->image_rows, g->img_height);
+    if (g->border_mode != TP_BORDER_REFERENCE && g->border_mode != TP_BORDER_CLAMP)
+        return fail(TP_ERR_GEOMETRY, "border_mode %d", g->border_mode);
+    out->W = g->img_width;
+    out->H = g->img_height;
+    out->TX = g->img_width / 8;
+    out->TY = g->img_height / 8;
+    out->TYA = (out->TY + 3) & ~3;
+    out->KH = g->kernels_hor;
+    out->KV = g->kernels_vert;
+    out->ls = g->kernels_lstep;
+    out->image_rows = g->image_rows;
+    out->border_mode = g->border_mode;
+    out->debug_marks = g->debug_marks ? 1 : 0;
+    return TP_OK;
+}
+
+int sm_count(int *n)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(TP_ERR_NO_DEVICE, "cudaGetDevice: %s", cudaGetErrorString(e));
+    e = cudaDeviceGetAttribute(n, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return fail(TP_ERR_NO_DEVICE, "SM count: %s", cudaGetErrorString(e));
+    return TP_OK;
+}
+
+/* blocks for a grid-stride kernel: enough to fill every SM `per_sm` times */
+unsigned grid_for(long long items, int items_per_block, int sms, int per_sm)
+{
+    long long need = (items + items_per_block - 1) / items_per_block;
+    long long cap = (long long)sms * per_sm;
+    if (need > cap) need = cap;
+    if (need < 1) need = 1;
+    return (unsigned)need;
+}
+
+/* host copy of the low-pass tables (last values set by tp_set_lpf) */
+float g_lpf_host[6][64] = TP_LPF_DEFAULT_INIT;
+const float g_lpf_default[6][64] = TP_LPF_DEFAULT_INIT;
+
+} /* namespace */
+
+extern "C" {
+
+const char *tp_last_error(void) { return g_err; }
+const char *tp_version(void) { return TP_VERSION; }
+
+int tp_tiles_x(const tp_geometry *g) { return g ? g->img_width / 8 : 0; }
+int tp_tiles_y(const tp_geometry *g) { return g ? g->img_height / 8 : 0; }
+int tp_tiles_ya(const tp_geometry *g) { return g ? ((g->img_height / 8 + 3) & ~3) : 0; }
+
+int tp_set_lpf(int which, const float *values)
+{
+    if (which < 0 || which > 5 || !values) return fail(TP_ERR_ARG, "tp_set_lpf(%d, %p)", which, values);
+    int rc = cuda_status(cudaMemcpyToSymbol(tp::c_lpf, values, 64 * sizeof(float), which * 64 * sizeof(float)),
+                         "cudaMemcpyToSymbol(lpf)");
+    if (rc) return rc;
+    memcpy(g_lpf_host[which], values, 64 * sizeof(float));
+    return TP_OK;
+}
+
+int tp_get_lpf(int which, float *values)
+{
+    if (which < 0 || which > 5 || !values) return fail(TP_ERR_ARG, "tp_get_lpf(%d, %p)", which, values);
+    memcpy(values, g_lpf_host[which], 64 * sizeof(float));
+    return TP_OK;
+}
+
+int tp_reset_lpf(void)
+{
+    for (int w = 0; w < 6; w++) {
+        int rc = tp_set_lpf(w, g_lpf_default[w]);
+        if (rc) return rc;
+    }
+    return TP_OK;
+}
+
+int tp_convert_correct_tiles(const tp_geometry *g, float *const *kernel_offsets, float *const *kernels,
+                             float *const *images, const tp_task *tasks, float *const *clt, size_t dstride,
+                             int num_tiles, int lpf_mask, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (!kernel_offsets || !kernels || !images || !clt) return fail(TP_ERR_ARG, "NULL pointer array");
+    if (num_tiles < 0) return fail(TP_ERR_ARG, "num_tiles %d < 0", num_tiles);
+    if (num_tiles > 0 && !tasks) return fail(TP_ERR_ARG, "tasks is NULL");
+    if (dstride < (size_t)g->img_width) return fail(TP_ERR_ARG, "dstride %zu < width %d", dstride, g->img_width);
+    if (num_tiles == 0) return TP_OK;
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    const long long warps = (long long)((num_tiles + 3) / 4) * 12;
+    unsigned grid = grid_for(warps, 8, sms, 8);
+    tp::k_convert_correct_tiles<<<grid, 256, 0, (cudaStream_t)stream>>>(
+        gd, dstride, kernel_offsets, kernels, images, tasks, clt, num_tiles, lpf_mask);
+    return cuda_status(cudaGetLastError(), "convert_correct_tiles launch");
+}
+
+int tp_correlate2D(const tp_geometry *g, float *const *clt, int colors, float scale0, float scale1,
+                   float scale2, float fat_zero, size_t num_corr_tiles, const int *corr_indices,
+                   size_t corr_stride, int corr_radius, float *corrs, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (!clt) return fail(TP_ERR_ARG, "clt is NULL");
+    if (colors != 1 && colors != 3) return fail(TP_ERR_ARG, "colors %d (1 or 3)", colors);
+    if (corr_radius < 0 || corr_radius > TP_MAX_CORR_RADIUS)
+        return fail(TP_ERR_ARG, "corr_radius %d outside 0..%d", corr_radius, TP_MAX_CORR_RADIUS);
+    const size_t sz = (size_t)(2 * corr_radius + 1) * (2 * corr_radius + 1);
+    if (num_corr_tiles == 0) return TP_OK;
+    if (!corr_indices || !corrs) return fail(TP_ERR_ARG, "NULL corr_indices / corrs");
+    if (corr_stride < sz) return fail(TP_ERR_ARG, "corr_stride %zu < (2r+1)^2 = %zu", corr_stride, sz);
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    unsigned grid = grid_for((long long)num_corr_tiles, 32, sms, 8);
+    tp::k_correlate2D<<<grid, 256, 0, (cudaStream_t)stream>>>(gd, clt, colors, scale0, scale1, scale2, fat_zero,
+                                                              (long long)num_corr_tiles, corr_indices,
+                                                              corr_stride, corr_radius, corrs);
+    return cuda_status(cudaGetLastError(), "correlate2D launch");
+}
+
+static int texture_params(int colors, float min_shot, float scale_shot, float diff_sigma, float w0, float w1,
+                          float w2, int dust_remove, int keep_weights, tp::TextureParams *p)
+{
+    if (colors != 1 && colors != 3) return fail(TP_ERR_ARG, "colors %d (1 or 3)", colors);
+    if (!(diff_sigma > 0.0f)) return fail(TP_ERR_ARG, "diff_sigma %g must be > 0", (double)diff_sigma);
+    if (scale_shot > 0.0f && !(min_shot > 0.0f))
+        return fail(TP_ERR_ARG, "min_shot %g must be > 0 when scale_shot > 0", (double)min_shot);
+    p->colors = colors;
+    p->min_shot = min_shot;
+    p->scale_shot = scale_shot;
+    p->diff_sigma = diff_sigma;
+    p->w0 = w0;
+    p->w1 = w1;
+    p->w2 = w2;
+    p->dust_remove = dust_remove;
+    p->keep_weights = keep_weights;
+    return TP_OK;
+}
+
+int tp_textures_accumulate(const tp_geometry *g, const int *woi, float *const *clt, size_t num_texture_tiles,
+                           const int *texture_indices, const float *port_offsets, int colors, int is_lwir,
+                           float min_shot, float scale_shot, float diff_sigma, float diff_threshold,
+                           float min_agree, float weight0, float weight1, float weight2, int dust_remove,
+                           int keep_weights, size_t texture_rbg_stride, float *texture_rbg,
+                           size_t texture_stride, float *texture_tiles, tp_stream_t stream)
+{
+    (void)is_lwir; (void)diff_threshold; (void)min_agree; /* accepted, unused (as in the reference) */
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    tp::TextureParams p;
+    if ((rc = texture_params(colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2, dust_remove,
+                             keep_weights, &p)))
+        return rc;
+    if (num_texture_tiles == 0) return TP_OK;
+    if (!clt || !texture_indices || !port_offsets) return fail(TP_ERR_ARG, "NULL clt / indices / port_offsets");
+    const bool want_rbg = texture_rbg && texture_rbg_stride;
+    const bool want_tiles = texture_tiles && texture_stride;
+    if (want_rbg && !woi) return fail(TP_ERR_ARG, "woi is NULL with an RGBA image output");
+    const int ns = (colors == 3) ? (keep_weights ? 12 : 4) : (keep_weights ? 8 : 2);
+    if (want_tiles && texture_stride < (size_t)ns * 256)
+        return fail(TP_ERR_ARG, "texture_stride %zu < %d slices x 256", texture_stride, ns);
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, 5);
+    tp::k_textures<<<grid, 128, 0, (cudaStream_t)stream>>>(
+        gd, woi, clt, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
+        want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
+        want_tiles ? texture_tiles : nullptr);
+    return cuda_status(cudaGetLastError(), "textures_accumulate launch");
+}
+
+int tp_imclt_rbg(const tp_geometry *g, const float *clt_one_cam, float *rbg, int color, int v_offset,
+                 int h_offset, size_t dstride, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (!clt_one_cam || !rbg) return fail(TP_ERR_ARG, "NULL clt / rbg");
+    if (color < 0 || color > 2) return fail(TP_ERR_ARG, "color %d outside 0..2", color);
+    if ((v_offset & ~1) || (h_offset & ~1)) return fail(TP_ERR_ARG, "offsets must be 0 or 1");
+    if (dstride < (size_t)g->img_width + 8) return fail(TP_ERR_ARG, "dstride %zu < width + 8", dstride);
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    const long long ntl = (long long)((gd.TX + (h_offset ^ 1)) >> 1) * ((gd.TY + (v_offset ^ 1)) >> 1);
+    unsigned grid = grid_for(ntl, 32, sms, 8);
+    tp::k_imclt_rbg<<<grid, 256, 0, (cudaStream_t)stream>>>(gd, clt_one_cam, rbg, color, v_offset, h_offset,
+                                                            dstride);
+    return cuda_status(cudaGetLastError(), "imclt_rbg launch");
+}
+
+int tp_imclt_rbg_all(const tp_geometry *g, const float *clt_one_cam, float *rbg, size_t dstride,
+                     tp_stream_t stream)
+{
+    for (int color = 0; color < 3; color++)
+        for (int v = 0; v < 2; v++)
+            for (int h = 0; h < 2; h++) {
+                int rc = tp_imclt_rbg(g, clt_one_cam, rbg, color, v, h, dstride, stream);
+                if (rc) return rc;
+            }
+    return TP_OK;
+}
+
+int tp_prepare_texture_list(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                            int *num_texture_tiles, int *woi, int width, int height, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (num_tiles < 0) return fail(TP_ERR_ARG, "num_tiles %d < 0", num_tiles);
+    if ((num_tiles > 0 && !tasks) || !texture_indices || !num_texture_tiles || !woi)
+        return fail(TP_ERR_ARG, "NULL tasks / texture_indices / num_texture_tiles / woi");
+    if (width < 0 || height < 0 || width > gd.TX || height > gd.TY)
+        return fail(TP_ERR_ARG, "list extent %dx%d outside %dx%d tiles", width, height, gd.TX, gd.TY);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long cap = (long long)gd.TX * gd.TYA;
+    if (height > 0) {
+        dim3 b0((width + 1 + 255) / 256, height, 1);
+        tp::k_clear_texture_list<<<b0, 256, 0, s>>>(texture_indices, width, height, gd.TX, cap);
+    }
+    const unsigned bt = (unsigned)((num_tiles + 255) / 256);
+    if (bt) tp::k_mark_texture_tiles<<<bt, 256, 0, s>>>(tasks, num_tiles, texture_indices, gd.TX, cap);
+    tp::k_woi_init<<<1, 32, 0, s>>>(woi, num_texture_tiles, gd.TX, gd.TY);
+    if (bt) {
+        tp::k_mark_neighbor_tiles<<<bt, 256, 0, s>>>(tasks, num_tiles, texture_indices, woi, gd.TX, gd.TY, cap);
+        tp::k_gen_texture_list<<<bt, 256, 0, s>>>(tasks, num_tiles, texture_indices, num_texture_tiles, woi,
+                                                  gd.TX, gd.TX * (gd.TYA >> 2), cap);
+    }
+    tp::k_woi_finalize<<<1, 32, 0, s>>>(woi);
+    return cuda_status(cudaGetLastError(), "prepare_texture_list launch");
+}
+
+int tp_clear_texture_rbga(const tp_geometry *g, int texture_width, int texture_slice_height,
+                          size_t texture_rbga_stride, float *texture_tiles, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (!texture_tiles) return fail(TP_ERR_ARG, "texture_tiles is NULL");
+    if (texture_width < 0 || texture_slice_height < 0) return fail(TP_ERR_ARG, "negative extent");
+    if (texture_rbga_stride < (size_t)texture_width) return fail(TP_ERR_ARG, "stride < width");
+    if (texture_width == 0 || texture_slice_height == 0) return TP_OK;
+    dim3 grid((unsigned)((texture_width + 8 + 255) / 256), (unsigned)(texture_slice_height < 65535 ? texture_slice_height : 65535), 1);
+    tp::k_clear_rbga<<<grid, 256, 0, (cudaStream_t)stream>>>(nullptr, 0, texture_width, texture_slice_height,
+                                                             texture_rbga_stride, texture_tiles);
+    return cuda_status(cudaGetLastError(), "clear_texture_rbga launch");
+}
+
+int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                     int *num_texture_tiles, int *woi, int width, int height, float *const *clt,
+                     const float *port_offsets, int colors, int is_lwir, float min_shot, float scale_shot,
+                     float diff_sigma, float diff_threshold, float min_agree, float weight0, float weight1,
+                     float weight2, int dust_remove, int keep_weights, size_t texture_rbga_stride,
+                     float *texture_tiles, tp_stream_t stream)
+{
+    (void)is_lwir; (void)diff_threshold; (void)min_agree; (void)keep_weights;
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    tp::TextureParams p;
+    if ((rc = texture_params(colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2, dust_remove, 0,
+                             &p)))
+        return rc;
+    if (!clt || !port_offsets || !texture_tiles) return fail(TP_ERR_ARG, "NULL clt / port_offsets / output");
+    if (texture_rbga_stride < (size_t)(gd.TX + 1) * 8)
+        return fail(TP_ERR_ARG, "texture_rbga_stride %zu < (tilesx + 1) * 8", texture_rbga_stride);
+    if ((rc = tp_prepare_texture_list(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height,
+                                      stream)))
+        return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    {
+        const int max_rows = (gd.TY + 1) * 8 * (colors + 1);
+        dim3 grid((unsigned)(((gd.TX + 2) * 8 + 255) / 256), (unsigned)(max_rows < 65535 ? max_rows : 65535), 1);
+        tp::k_clear_rbga<<<grid, 256, 0, s>>>(woi, colors, 0, 0, texture_rbga_stride, texture_tiles);
+    }
+    const int quarter = gd.TX * (gd.TYA >> 2);
+    const unsigned grid = grid_for(quarter, 1, sms, 5);
+    for (int pass = 0; pass < 8; pass++) {
+        const int border = pass >> 2;
+        const int slot = ((pass & 3) << 1) + border;
+        const int *base = texture_indices + (pass & 3) * quarter;
+        tp::k_textures<<<grid, 128, 0, s>>>(gd, woi, clt, 0, base, num_texture_tiles, slot, quarter,
+                                            border ? quarter : 0, port_offsets, p, texture_rbga_stride,
+                                            texture_tiles, 0, nullptr);
+    }
+    return cuda_status(cudaGetLastError(), "generate_RBGA launch");
+}
+
+} /* extern "C" */

@@ -1,0 +1,242 @@
+/*
+ * tp_convert.cuh - forward CLT with aberration correction (the drop-in for the
+ * reference's convert_correct_tiles, src/TileProcessor.cuh:1859-1937 and
+ * convertCorrectTile :3106-3635).
+ *
+ * One 8-lane group per (tile, camera, color) job; a warp holds four jobs of the
+ * same camera and color for four consecutive tasks, so the green jobs (two
+ * Bayer phases and a DST pass) never share a warp with the cheaper red/blue
+ * ones.  Per job:
+ *   lane u gathers DTT row u of the folded, windowed Bayer samples (one image
+ *   row, 8 same-color pixels), applies the row DCT-IV (green: also the row
+ *   DST-IV of the sine-windowed fold), transposes through shared memory and
+ *   applies the column DCT-IV, ending with column u of CC (and SC);
+ *   the remaining quadrants come from the Bayer mirror symmetries by lane
+ *   shuffles; the CLT-domain kernel, the two residual-shift rotations and the
+ *   optional LPF are per-coefficient and run in registers; the 256
+ *   coefficients are stored as 32-byte row segments.
+ */
+#pragma once
+#include "tp_common.cuh"
+
+namespace tp {
+
+/* Clamp of the integer tile corner (src/TileProcessor.cuh:3188-3193,
+ * :3246-3252); `n` is the image size along the axis. */
+__device__ __forceinline__ int corner_clamp(int itl, int n, bool horizontal, int mode)
+{
+    if (itl < 0) itl &= 1;
+    if (itl >= n - 8) {
+        if (mode == TP_BORDER_REFERENCE && horizontal)
+            itl = itl & (1 + (n - 8 - 2)); /* the reference's `itlx & 1 +(W-10)` */
+        else
+            itl = (itl & 1) + (n - 8 - 2);
+    }
+    return itl;
+}
+
+__device__ __forceinline__ int pair_clamp(int idx, int n)
+{
+    if (idx < 0) return idx & 1;
+    if (idx >= n) return (n - 2) + (idx & 1);
+    return idx;
+}
+
+struct ConvertJob {
+    int cam, color;
+};
+
+__device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
+                                            const float *__restrict__ extra_tab,
+                                            const float *__restrict__ kern_tab,
+                                            const float *__restrict__ img, float cx, float cy,
+                                            int color, int lpf_mask, float *__restrict__ out,
+                                            float (*tb)[9], int l, unsigned gm)
+{
+    /* ---- kernel tile, integer corner, residual shift (float32, as the
+     * reference computes them: src/TileProcessor.cuh:3129-3255) ---- */
+    const float step_inv = __int_as_float((127 - g.ls) << 23);
+    int ktx = __float2int_rn(__fmaf_rn(cx, step_inv, 1.0f));
+    int kty = __float2int_rn(__fmaf_rn(cy, step_inv, 1.0f));
+    ktx = min(g.KH - 1, max(0, ktx));
+    kty = min(g.KV - 1, max(0, kty));
+    const float kdx = (cx - (float)(ktx << g.ls)) + (float)(1 << (g.ls - 1));
+    const float kdy = (cy - (float)(kty << g.ls)) + (float)(1 << (g.ls - 1));
+    const size_t kidx = ((size_t)ktx + (size_t)kty * g.KH) * 3 + color;
+    const float *ex = extra_tab + kidx * 8;
+    const float data_x = __ldg(ex + 0), data_y = __ldg(ex + 1);
+    const float dxc_dx = __ldg(ex + 4), dxc_dy = __ldg(ex + 5);
+    const float dyc_dx = __ldg(ex + 6), dyc_dy = __ldg(ex + 7);
+    const float px = (cx - 8.0f) - __fmaf_rn(dxc_dy, kdy, __fmaf_rn(dxc_dx, kdx, data_x));
+    const float py = (cy - 8.0f) - __fmaf_rn(dyc_dy, kdy, __fmaf_rn(dyc_dx, kdx, data_y));
+    const int itlx = corner_clamp(__float2int_rd(px + 0.5f), g.W, true, g.border_mode);
+    const int itly = corner_clamp(__float2int_rd(py + 0.5f), g.H, false, g.border_mode);
+    const float shx = (float)itlx - px;
+    const float shy = (float)itly - py;
+
+    /* (cos, sin)(pi s / 16) for the shifted windows */
+    const float xh = shx * (1.0f / 16.0f), xv = shy * (1.0f / 16.0f);
+    const float hc = cospif(xh), hs = sinpif(xh);
+    const float vc = cospif(xv), vs = sinpif(xv);
+
+    const int c0 = color & 1, c1 = (color >> 1) & 1;
+    const bool fast = (itlx >= 0) && (itlx < g.W - 16) && (itly >= 0) && (itly < g.H - 16);
+    const long long last = (long long)g.image_rows * (long long)dstride - 1;
+
+    /* ---- fold: lane l builds DTT row l ---- */
+    float P[8], Q[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) { P[v] = 0.0f; Q[v] = 0.0f; }
+#pragma unroll
+    for (int gp = 0; gp < 2; gp++) {
+        if (gp > c1) break;
+        const int colp = (itlx & 1) ^ (1 ^ c0 ^ c1 ^ gp);
+        const int rowp = (itly & 1) ^ (c0 ^ gp);
+        const int lr = fold_sample(l, rowp);
+        const float wv = fold_sign_c(lr) * shifted_window(lr, vc, vs);
+        long long rowbase;
+        int eff_col = 0;
+        if (fast) {
+            rowbase = (long long)(itly + lr) * (long long)dstride + itlx;
+        } else if (g.border_mode == TP_BORDER_CLAMP) {
+            rowbase = (long long)pair_clamp(itly + lr, g.H) * (long long)dstride;
+        } else {
+            /* src/TileProcessor.cuh:3328-3361: columns clamped by IMG_HEIGHT/2,
+             * rows by IMG_WIDTH/2, row offset `rowp` added once */
+            const int i = (lr - rowp) >> 1;
+            int rp = min(g.W / 2 - 1, max(0, (itly >> 1) + i));
+            int cp = min(g.H / 2 - 1, max(0, itlx >> 1));
+            eff_col = (cp << 1) + (itlx & 1);
+            rowbase = (long long)(rowp + (rp << 1) + (itly & 1)) * (long long)dstride + eff_col;
+        }
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            const int lc = fold_sample(v, colp);
+            const float whs_raw = shifted_window(lc, hc, hs);
+            float pix;
+            if (fast) {
+                pix = __ldg(img + rowbase + lc);
+            } else if (g.border_mode == TP_BORDER_CLAMP) {
+                pix = __ldg(img + rowbase + pair_clamp(itlx + lc, g.W));
+            } else {
+                long long a = rowbase + lc;
+                a = a > last ? last : (a < 0 ? 0 : a);
+                pix = __ldg(img + a);
+            }
+            const float d = pix * wv;
+            P[v] = __fmaf_rn(d, fold_sign_c(lc) * whs_raw, P[v]);
+            if (c1) Q[v] = __fmaf_rn(d, fold_sign_s(lc) * whs_raw, Q[v]);
+        }
+    }
+
+    /* ---- 2-D transform: rows (registers), transpose, columns ---- */
+    float cc[8], sc[8], cs[8], ss[8], t[8];
+    dtt8<0>(P, t);
+    group_transpose(tb, t, P, l, gm);
+    dtt8<0>(P, cc); /* lane l: column l of CC */
+    if (c1) {
+        dtt8<1>(Q, t);
+        group_transpose(tb, t, Q, l, gm);
+        dtt8<0>(Q, sc); /* column l of SC */
+    } else {
+        /* R, B: SC[i][7-j] = +-CC[i][j] (src/TileProcessor.cuh:3459-3475) */
+        const float neg1 = 1.0f - 2.0f * (float)((itlx & 1) ^ (1 ^ color));
+#pragma unroll
+        for (int m = 0; m < 8; m++) sc[m] = neg1 * __shfl_xor_sync(gm, cc[m], 7);
+    }
+    /* SS[7-i][7-j] = +-CC[i][j], CS[7-i][7-j] = +-SC[i][j] (:3486-3504) */
+    const float neg2 = 1.0f - 2.0f * (float)((itlx & 1) ^ (itly & 1) ^ 1 ^ c1);
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        ss[m] = neg2 * __shfl_xor_sync(gm, cc[7 - m], 7);
+        cs[m] = neg2 * __shfl_xor_sync(gm, sc[7 - m], 7);
+    }
+
+    /* ---- CLT-domain convolution (src/TileProcessor.cuh:2778-2827) ---- */
+    const float *kr = kern_tab + kidx * 256 + l;
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const float k0 = __ldg(kr + m * 8), k1 = __ldg(kr + 64 + m * 8);
+        const float k2 = __ldg(kr + 128 + m * 8), k3 = __ldg(kr + 192 + m * 8);
+        const float a0 = cc[m], a1 = sc[m], a2 = cs[m], a3 = ss[m];
+        cc[m] = __fmaf_rn(a3, k3, __fmaf_rn(-a2, k2, __fmaf_rn(-a1, k1, a0 * k0)));
+        sc[m] = __fmaf_rn(-a2, k3, __fmaf_rn(-a3, k2, __fmaf_rn(a0, k1, a1 * k0)));
+        cs[m] = __fmaf_rn(-a1, k3, __fmaf_rn(a0, k2, __fmaf_rn(-a3, k1, a2 * k0)));
+        ss[m] = __fmaf_rn(a0, k3, __fmaf_rn(a1, k2, __fmaf_rn(a2, k1, a3 * k0)));
+    }
+
+    /* ---- residual shift: horizontal (this lane's column), then vertical
+     * (per row, angles shared across the group) (:2715-2776) ---- */
+    {
+        const float a = (shx * (float)(2 * l + 1)) * 0.0625f;
+        const float ch = cospif(a), sh = sinpif(a);
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const float x0 = cc[m], x1 = sc[m], x2 = cs[m], x3 = ss[m];
+            cc[m] = x0 * ch - x1 * sh;
+            sc[m] = x0 * sh + x1 * ch;
+            cs[m] = x2 * ch - x3 * sh;
+            ss[m] = x2 * sh + x3 * ch;
+        }
+    }
+    {
+        const float a = (shy * (float)(2 * l + 1)) * 0.0625f;
+        const float cvl = cospif(a), svl = sinpif(a);
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const float cv = __shfl_sync(gm, cvl, m, 8), sv = __shfl_sync(gm, svl, m, 8);
+            const float x0 = cc[m], x1 = sc[m], x2 = cs[m], x3 = ss[m];
+            cc[m] = x0 * cv - x2 * sv;
+            cs[m] = x0 * sv + x2 * cv;
+            sc[m] = x1 * cv - x3 * sv;
+            ss[m] = x1 * sv + x3 * cv;
+        }
+    }
+    if ((lpf_mask >> color) & 1) { /* optional LPF (:3572-3593) */
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const float f = c_lpf[color][m * 8 + l];
+            cc[m] *= f; sc[m] *= f; cs[m] *= f; ss[m] *= f;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        out[m * 8 + l] = cc[m];
+        out[64 + m * 8 + l] = sc[m];
+        out[128 + m * 8 + l] = cs[m];
+        out[192 + m * 8 + l] = ss[m];
+    }
+}
+
+/* Warp w of the grid-stride loop handles tasks 4*(w/12) .. +3 for camera
+ * (w%12)%4 and color (w%12)/4. */
+__global__ void __launch_bounds__(256, 2) k_convert_correct_tiles(
+    Geom g, size_t dstride, float *const *kernel_offsets, float *const *kernels,
+    float *const *images, const tp_task *__restrict__ tasks, float *const *clt, int num_tiles,
+    int lpf_mask)
+{
+    __shared__ float tbuf[256 / 8][8][9];
+    const int l = threadIdx.x & 7;
+    const int grp = threadIdx.x >> 3;
+    const unsigned gm = group_mask();
+    const int warps_total = gridDim.x * (blockDim.x >> 5);
+    const int chunks = (num_tiles + 3) >> 2;
+    for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < chunks * 12; w += warps_total) {
+        const int chunk = w / 12, r = w - chunk * 12;
+        const int color = r >> 2, cam = r & 3;
+        const int n = chunk * 4 + ((threadIdx.x >> 3) & 3);
+        if (n >= num_tiles) continue;
+        const tp_task *t = tasks + n;
+        const int task = t->task;
+        if (!task) continue;
+        const int txy = t->txy;
+        const int tx = txy & 0xfff, ty = txy >> 16;
+        if (tx >= g.TX || ty < 0 || ty >= g.TY) continue;
+        const float cx = t->xy[cam][0], cy = t->xy[cam][1];
+        float *out = clt[cam] + (((size_t)ty * g.TX + tx) * 3 + color) * 256;
+        convert_job(g, dstride, kernel_offsets[cam], kernels[cam], images[cam], cx, cy, color,
+                    lpf_mask, out, tbuf[grp], l, gm);
+    }
+}
+
+} /* namespace tp */

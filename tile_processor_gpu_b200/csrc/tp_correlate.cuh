@@ -1,0 +1,133 @@
+/*
+ * tp_correlate.cuh - pairwise phase correlation (the drop-in for the
+ * reference's correlate2D, src/TileProcessor.cuh:1176-1443, with its helpers
+ * correlateAccumulateTiles :2829-2890, normalizeTileAmplitude :2915-2942 and
+ * corrUnfoldTile :2950-3008).
+ *
+ * One 8-lane group per (tile, pair) entry of the index list.  Lane l holds
+ * column l of the four accumulated quadrants; the color accumulation, the two
+ * LPFs and the amplitude normalisation are per coefficient; the vertical
+ * DCT-II/DST-II runs on the held column, one shared-memory transpose per
+ * quadrant gives rows for the horizontal pass, and the unfold into the
+ * (2r+1)^2 output takes the previous row of quadrants 2 and 3 from the lane
+ * above by a shuffle.  The output tile is staged in shared memory and written
+ * as consecutive floats.
+ */
+#pragma once
+#include "tp_common.cuh"
+
+namespace tp {
+
+__global__ void __launch_bounds__(256) k_correlate2D(Geom g, float *const *clt, int colors,
+                                                     float scale0, float scale1, float scale2,
+                                                     float fat_zero, long long num_corr_tiles,
+                                                     const int *__restrict__ corr_indices,
+                                                     size_t corr_stride, int corr_radius,
+                                                     float *__restrict__ corrs)
+{
+    __shared__ float tbuf[256 / 8][kTB4];
+    const int l = threadIdx.x & 7;
+    const int grp = threadIdx.x >> 3;
+    const unsigned gm = group_mask();
+    const long long groups_total = (long long)gridDim.x * (blockDim.x >> 3);
+    const int ntiles = g.TX * g.TY;
+    const int r = corr_radius, sz = 2 * r + 1;
+    float *tb = tbuf[grp];
+    for (long long n = (long long)blockIdx.x * (blockDim.x >> 3) + grp; n < num_corr_tiles; n += groups_total) {
+        const int code = corr_indices[n];
+        const int tile = code >> 8, pair = code & 0xff;
+        if (pair >= 6 || tile < 0 || tile >= ntiles) continue;
+        const float *ta = clt[c_pairs[pair][0]] + (size_t)tile * 768 + l;
+        const float *tb2 = clt[c_pairs[pair][1]] + (size_t)tile * 768 + l;
+        float acc[4][8];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int m = 0; m < 8; m++) acc[q][m] = 0.0f;
+        for (int color = 0; color < colors; color++) {
+            const float s = color == 0 ? scale0 : color == 1 ? scale1 : scale2;
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const int o = color * 256 + m * 8;
+                const float a0 = __ldg(ta + o), a1 = __ldg(ta + o + 64), a2 = __ldg(ta + o + 128), a3 = __ldg(ta + o + 192);
+                const float b0 = __ldg(tb2 + o), b1 = __ldg(tb2 + o + 64), b2 = __ldg(tb2 + o + 128), b3 = __ldg(tb2 + o + 192);
+                /* CLT-domain correlation of the two tiles */
+                const float r0 = __fmaf_rn(a3, b3, __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, a0 * b0)));
+                const float r1 = __fmaf_rn(a2, b3, __fmaf_rn(-a3, b2, __fmaf_rn(a0, b1, -a1 * b0)));
+                const float r2 = __fmaf_rn(a1, b3, __fmaf_rn(a0, b2, __fmaf_rn(-a3, b1, -a2 * b0)));
+                const float r3 = __fmaf_rn(a0, b3, __fmaf_rn(-a1, b2, __fmaf_rn(-a2, b1, a3 * b0)));
+                acc[0][m] = __fmaf_rn(s, r0, acc[0][m]);
+                acc[1][m] = __fmaf_rn(s, r1, acc[1][m]);
+                acc[2][m] = __fmaf_rn(s, r2, acc[2][m]);
+                acc[3][m] = __fmaf_rn(s, r3, acc[3][m]);
+            }
+            if (color == 1) { /* LPF after red and blue */
+#pragma unroll
+                for (int m = 0; m < 8; m++) {
+                    const float f = c_lpf[4][m * 8 + l];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[q][m] *= f;
+                }
+            }
+        }
+        /* amplitude normalisation with fat zero, then the final LPF */
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            float s2 = fat_zero * fat_zero;
+#pragma unroll
+            for (int q = 0; q < 4; q++) s2 = __fmaf_rn(acc[q][m], acc[q][m], s2);
+            const float sc = rsqrtf(s2);
+            const float f = c_lpf[5][m * 8 + l];
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q][m] = (acc[q][m] * sc) * f;
+        }
+        /* pixel domain: vertical DCT-II (q0,q1) / DST-II (q2,q3) on the held
+         * column, transpose, horizontal DCT-II (q0,q2) / DST-II (q1,q3) */
+        float pix[4][8];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            float v[8], row[8];
+            if (q >> 1) dtt8<3>(acc[q], v); else dtt8<2>(acc[q], v);
+#pragma unroll
+            for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
+            __syncwarp(gm);
+#pragma unroll
+            for (int k = 0; k < 8; k++) row[k] = tb[TBI(q, k, l)];
+            __syncwarp(gm);
+            if (q & 1) dtt8<3>(row, pix[q]); else dtt8<2>(row, pix[q]);
+        }
+        /* unfold (lane i = row i): R[+-i][+-j] from q0[i][j], q1[i][j-1],
+         * q2[i-1][j], q3[i-1][j-1] */
+        float p2u[8], p3u[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            p2u[k] = __shfl_up_sync(gm, pix[2][k], 1, 8);
+            p3u[k] = __shfl_up_sync(gm, pix[3][k], 1, 8);
+        }
+        float *stage = tb; /* 296 floats >= 225 */
+        if (l <= r) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                if (j > r) break;
+                const float q0 = pix[0][j];
+                const float q1 = j > 0 ? pix[1][j - 1] : 0.0f;
+                const float q2 = l > 0 ? p2u[j] : 0.0f;
+                const float q3 = (l > 0 && j > 0) ? p3u[j - 1] : 0.0f;
+                const float pp = 0.25f * ((q0 + q1) + (q2 + q3));
+                const float pm = 0.25f * ((q0 - q1) + (q2 - q3));
+                const float mp = 0.25f * ((q0 + q1) - (q2 + q3));
+                const float mm = 0.25f * ((q0 - q1) - (q2 - q3));
+                stage[(r + l) * sz + (r + j)] = pp;
+                stage[(r + l) * sz + (r - j)] = pm;
+                stage[(r - l) * sz + (r + j)] = mp;
+                stage[(r - l) * sz + (r - j)] = mm;
+            }
+        }
+        __syncwarp(gm);
+        float *dst = corrs + (size_t)n * corr_stride;
+        for (int k = l; k < sz * sz; k += 8) dst[k] = stage[k];
+        __syncwarp(gm);
+    }
+}
+
+} /* namespace tp */
