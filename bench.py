@@ -1,0 +1,415 @@
+"""Benchmark: full-frame quad-camera CLT + correlation + texture, frames/s.
+
+One step = one 2592x1936 quad-camera Bayer frame (78,408 tiles) through the
+hot path, on inputs already resident in HBM:
+  1. tp_convert_correct_tiles  forward CLT + aberration kernels + shifts
+  2. tp_correlate2D            6 camera pairs per tile, 15x15 outputs
+  3. tp_generate_RBGA          texture list + overlapped RGBA texture
+`value` is whole-job frames/s (N GPUs each process their own frames:
+frame-level replicas, weak scaling).  `e2e` is the same pipeline driven
+through the public API with host buffers: each step copies the frame's four
+images from pinned host memory and reads the correlation tiles and the RGBA
+texture back.
+
+`--impl reference` times the CPU implementation (the FP64 port of the
+reference's tile math, all host threads) on a bounded sample of the same
+workload.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WIDTH, HEIGHT = 2592, 1936
+METRIC = "quad 5MP frames/s (CLT+corr+texture)"
+UNIT = "frames/s"
+CORR_RADIUS = 7
+FAT_ZERO = 0.05
+TEXTURE = dict(colors=3, is_lwir=0, min_shot=10.0, scale_shot=3.0, diff_sigma=1.5, diff_threshold=10.0,
+               min_agree=3.0, weight0=0.294118, weight1=0.117647, weight2=0.588235, dust_remove=1, keep_weights=0)
+WORKLOAD = ("full-frame quad 2592x1936 Bayer (78,408 tiles): convert_correct_tiles + correlate2D "
+            "(6 pairs, 15x15) + generate_RBGA (texture list + overlapped RGBA)")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return rank, world, local, pg
+
+
+def max_over_ranks(pg, value):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# --------------------------------------------------------------------------- #
+# the B200 pipeline
+# --------------------------------------------------------------------------- #
+class FramePipeline:
+    """Device buffers for one frame and the three hot-path calls."""
+
+    def __init__(self, seed=0, device="cuda"):
+        import torch
+        from tile_processor_gpu_b200 import api, synth
+        self.api, self.torch = api, torch
+        rng = np.random.default_rng(seed)
+        self.geom_d = synth.geometry(WIDTH, HEIGHT, image_rows=HEIGHT + 16)
+        g = self.g = api.Geometry.from_dict(self.geom_d)
+        self.TX, self.TY, self.TYA = synth.tiles(self.geom_d)
+        imgs, disp = synth.plane_scene(rng, WIDTH, HEIGHT, disparity=(0.0, 64.0))
+        self.dstride = WIDTH + 64
+        pitched = np.zeros((4, HEIGHT + 16, self.dstride), np.float32)
+        pitched[:, :HEIGHT, :WIDTH] = imgs
+        self.host_images = [torch.from_numpy(pitched[c]).pin_memory() for c in range(4)]
+        kern, extra = synth.kernel_tables(rng, self.geom_d, pool=256)
+        self.tasks_np = synth.tasks_grid(self.geom_d, rng, jitter=0.5, disparity=disp)
+        self.num_tiles = int(self.tasks_np.size)
+        self.images = [h.to(device) for h in self.host_images]
+        self.kernels = [torch.from_numpy(kern[c]).to(device) for c in range(4)]
+        self.extra = [torch.from_numpy(extra[c]).to(device) for c in range(4)]
+        self.tasks = api.tasks_to_device(self.tasks_np, device)
+        self.clt = [torch.empty(self.TY * self.TX * 768, dtype=torch.float32, device=device) for _ in range(4)]
+        self.p_images, self.p_kernels = api.PointerArray(self.images), api.PointerArray(self.kernels)
+        self.p_extra, self.p_clt = api.PointerArray(self.extra), api.PointerArray(self.clt)
+        corr_idx = synth.corr_indices_fast(self.tasks_np, self.geom_d)
+        self.num_corr = int(corr_idx.size)
+        self.corr_idx = torch.from_numpy(corr_idx).to(device)
+        self.corr_size = (2 * CORR_RADIUS + 1) ** 2
+        self.corr_stride = self.corr_size
+        self.corrs = torch.empty((self.num_corr, self.corr_stride), dtype=torch.float32, device=device)
+        self.tex_indices = torch.empty(self.TX * self.TYA, dtype=torch.int32, device=device)
+        self.num_tex = torch.empty(8, dtype=torch.int32, device=device)
+        self.woi = torch.empty(4, dtype=torch.int32, device=device)
+        self.rgba_stride = (self.TX + 1) * 8
+        self.rgba_rows = (self.TY + 1) * 8 * (TEXTURE["colors"] + 1)
+        self.rgba = torch.empty((self.rgba_rows, self.rgba_stride), dtype=torch.float32, device=device)
+        self.port_offsets = torch.from_numpy(synth.PORT_OFFSETS.reshape(-1).copy()).to(device)
+        # kernel-table bytes a frame touches (distinct kernel tiles of all jobs)
+        self.kernel_tiles_touched = self._touched_kernel_tiles()
+        self.host_corrs = torch.empty_like(self.corrs, device="cpu").pin_memory()
+        self.host_rgba = torch.empty_like(self.rgba, device="cpu").pin_memory()
+
+    def _touched_kernel_tiles(self):
+        gd = self.geom_d
+        n = 0
+        for cam in range(4):
+            cx = self.tasks_np["xy"][:, cam, 0].astype(np.float32)
+            cy = self.tasks_np["xy"][:, cam, 1].astype(np.float32)
+            kx = np.clip(np.rint(cx / 16 + 1), 0, gd["kernels_hor"] - 1).astype(np.int64)
+            ky = np.clip(np.rint(cy / 16 + 1), 0, gd["kernels_vert"] - 1).astype(np.int64)
+            n += np.unique(kx + ky * gd["kernels_hor"]).size * 3
+        return n
+
+    # stage calls (each is a C ABI call on the current stream)
+    def convert(self):
+        self.api.convert_correct_tiles(self.g, self.p_extra, self.p_kernels, self.p_images, self.tasks, self.p_clt,
+                                       self.dstride, self.num_tiles, 0)
+
+    def correlate(self):
+        self.api.correlate2D(self.g, self.p_clt, 3, 0.25, 0.25, 0.5, FAT_ZERO, self.num_corr, self.corr_idx,
+                             self.corr_stride, CORR_RADIUS, self.corrs)
+
+    def texture(self):
+        t = TEXTURE
+        self.api.generate_RBGA(self.g, self.tasks, self.num_tiles, self.tex_indices, self.num_tex, self.woi, self.TX,
+                               self.TY, self.p_clt, self.port_offsets, t["colors"], t["is_lwir"], t["min_shot"],
+                               t["scale_shot"], t["diff_sigma"], t["diff_threshold"], t["min_agree"], t["weight0"],
+                               t["weight1"], t["weight2"], t["dust_remove"], 0, self.rgba_stride, self.rgba)
+
+    STAGES = ("convert", "correlate", "texture")
+    LAUNCHES = {"convert": 1, "correlate": 1, "texture": 15}
+
+    def step(self):
+        self.convert()
+        self.correlate()
+        self.texture()
+
+    def algorithmic_bytes(self):
+        """compulsory HBM bytes of each stage of one frame"""
+        T = self.num_tiles
+        clt = 4 * T * 3 * 1024
+        return {
+            "convert": 4 * WIDTH * HEIGHT * 4 + self.kernel_tiles_touched * (1024 + 32) + T * 40 + clt,
+            "correlate": clt + self.num_corr * 4 + self.num_corr * self.corr_size * 4,
+            "texture": clt + T * 40 + (self.TX + 1) * 8 * (self.TY + 1) * 8 * 4 * 4,
+        }
+
+
+def run_b200(args, rank, world, local, pg):
+    import torch
+    dev = "cuda:%d" % local
+    torch.cuda.set_device(local)
+    from tile_processor_gpu_b200 import build
+    build.build()
+    pipe = FramePipeline(seed=100 + rank, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        pipe.step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev = {s: [] for s in pipe.STAGES}
+    barrier(pg)
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for _ in range(args.steps):
+        for s in pipe.STAGES:
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            getattr(pipe, s)()
+            b.record(stream)
+            ev[s].append((a, b))
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    clocks = sampler.stop()
+    ms = t_start.elapsed_time(t_end)
+    ms_max = max_over_ranks(pg, ms)
+    stage_ms = {s: sum(a.elapsed_time(b) for a, b in ev[s]) / args.steps for s in pipe.STAGES}
+
+    # ---- end to end through the public API with host buffers ----
+    e2e_steps = max(2, min(args.steps, 10))
+    h2d = sum(h.numel() * 4 for h in pipe.host_images)
+    d2h = pipe.corrs.numel() * 4 + pipe.rgba.numel() * 4
+    barrier(pg)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        for c in range(4):
+            pipe.images[c].copy_(pipe.host_images[c], non_blocking=True)
+        pipe.step()
+        pipe.host_corrs.copy_(pipe.corrs, non_blocking=True)
+        pipe.host_rgba.copy_(pipe.rgba, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    e2e_ms = max_over_ranks(pg, e0.elapsed_time(e1)) / e2e_steps
+
+    if rank != 0:
+        return None
+    hbm, peak_kind = peaks()
+    dom = max(stage_ms, key=stage_ms.get)
+    algo = pipe.algorithmic_bytes()
+    achieved = algo[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    fps = world * args.steps / (ms_max * 1e-3)
+    out = {
+        "metric": METRIC, "value": round(fps, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plane scene, PSF kernels)",
+        "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "tiles": pipe.num_tiles,
+                   "corr_tiles": pipe.num_corr, "parallelism": "frame replicas x%d" % world,
+                   "l2": "per-step working set %.2f GB > 126 MB L2 (no flush)" % (sum(algo.values()) / 1e9)},
+        "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes": int(algo[dom]), "traffic": None},
+        "e2e": {"value": round(world / (e2e_ms * 1e-3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(args.steps * sum(pipe.LAUNCHES.values())),
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.cpu_sample_tiles)
+    return out
+
+
+# --------------------------------------------------------------------------- #
+# CPU implementation (the FP64 port of the reference's tile math)
+# --------------------------------------------------------------------------- #
+def cpu_pipeline(sample_tiles, seed=0):
+    """A bounded sample of the workload for the CPU port: a crop of the same
+    seeded scene, sized to about `sample_tiles` tiles, through all three
+    stages (the per-tile work does not depend on the frame size)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from tile_processor_gpu_b200 import synth
+    O.build()
+    rng = np.random.default_rng(seed)
+    w = WIDTH
+    h = max(32, min(HEIGHT, (sample_tiles // (WIDTH // 8)) * 8))
+    geom = synth.geometry(w, h, image_rows=h + 16)
+    imgs, disp = synth.plane_scene(rng, w, h, disparity=(0.0, 64.0))
+    dstride = w + 64
+    pitched = np.zeros((4, h + 16, dstride), np.float32)
+    pitched[:, :h, :w] = imgs
+    kern, extra = synth.kernel_tables(rng, geom, pool=256)
+    tasks = synth.tasks_grid(geom, rng, jitter=0.5, disparity=disp)
+    corr_idx = synth.corr_indices_fast(tasks, geom)
+    TX, TY, _ = synth.tiles(geom)
+
+    def step():
+        clt = O.convert_correct_tiles(geom, extra, kern, pitched, dstride, tasks)
+        O.correlate2D(geom, clt, 3, .25, .25, .5, FAT_ZERO, corr_idx, (2 * CORR_RADIUS + 1) ** 2, CORR_RADIUS)
+        O.generate_RBGA(geom, tasks, TX, TY, clt, synth.PORT_OFFSETS, (TX + 1) * 8, (TY + 1) * 8 * 4 + 8)
+
+    return O, step, int(tasks.size), "%dx%d crop (%d tiles)" % (w, h, tasks.size)
+
+
+def cpu_baseline(sample_tiles, min_seconds=10.0, max_reps=5):
+    """The port on all host threads: repeat the sample until about
+    `min_seconds` of CPU work (at most `max_reps` repetitions)."""
+    O, step, ntiles, what = cpu_pipeline(sample_tiles)
+    reps = 0
+    t = time.perf_counter()
+    while reps < max_reps and (reps == 0 or time.perf_counter() - t < min_seconds):
+        step()
+        reps += 1
+    dt = (time.perf_counter() - t) / reps
+    frames = ntiles / ((WIDTH // 8) * (HEIGHT // 8))
+    return {"value": round(frames / dt, 5), "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+            "sample": "%s of the scene through all three stages, FP64, %d rep(s); frames = tiles / 78,408" % (
+                what, reps)}
+
+
+def run_reference(args, rank, world, pg):
+    if rank != 0:
+        return None
+    O, step, ntiles, what = cpu_pipeline(args.cpu_sample_tiles)
+    for _ in range(args.warmup):
+        step()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t) / args.steps
+    frames = ntiles / ((WIDTH // 8) * (HEIGHT // 8))
+    v = frames / dt
+    return {
+        "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 / v, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded plane scene, PSF kernels)",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT),
+                   "sample_tiles_per_step": ntiles, "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+                         "sample": "%s per step through all three stages, FP64; frames = tiles / 78,408" % what},
+        "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-sample-tiles", type=int, default=20000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # CPU arm: rank 0 alone runs it, the other ranks exit without work
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank, world, None)))
+        return
+    rank, world, local, pg = dist_setup(args)
+    try:
+        out = run_b200(args, rank, world, local, pg)
+        if rank == 0 and out is not None:
+            print(json.dumps(out))
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -667,36 +667,38 @@ int tpo_textures_accumulate(const tp_geometry *g, const int *woi, const double *
     const int TX = tiles_x(g), ntiles = TX * tiles_y(g);
     const int nslices_tile = (colors == 3) ? (keep_weights ? 12 : 4) : (keep_weights ? 8 : 2);
     const int nslices_img = colors + 1;
-    /* tiles of one list never overlap in the image only within one parity
-     * pass, so the overlap-add below is done serially in list order */
+    /* tiles are computed in parallel in chunks; the overlap-add of a chunk
+     * runs serially in list order (tiles of one list may overlap) */
     int done = 0;
-    double (*outs)[12][16][16] = (double (*)[12][16][16])malloc(sizeof(double) * 12 * 256 *
-                                                               (size_t)(num_texture_tiles > 0 ? num_texture_tiles : 1));
+    const int chunk = 2048;
+    double (*outs)[12][16][16] = (double (*)[12][16][16])malloc(sizeof(double) * 12 * 256 * (size_t)chunk);
+    const size_t slice_stride = texture_rbg_stride * (size_t)((woi ? woi[3] : 0) + 1) * 8;
+    for (int n0 = 0; n0 < num_texture_tiles; n0 += chunk) {
+        const int n1 = (n0 + chunk < num_texture_tiles) ? n0 + chunk : num_texture_tiles;
+        int valid[2048];
 #pragma omp parallel for schedule(dynamic, 4) reduction(+ : done) num_threads(tpo_get_threads())
-    for (int n = 0; n < num_texture_tiles; n++) {
-        int code = texture_indices[n];
-        if (!(code & (1 << 7))) continue;
-        int tile = code >> 8;
-        if (tile < 0 || tile >= ntiles) continue;
-        texture_tile(tile, clt, colors, lpf, min_shot, scale_shot, port_offsets, diff_sigma, chw,
-                     dust_remove, keep_weights, outs[n], margin ? margin + (size_t)n * 256 : NULL);
-        if (texture_tiles && texture_stride) {
-            double *dst = texture_tiles + (size_t)n * texture_stride;
-            for (int s = 0; s < nslices_tile; s++) {
-                /* colors==1 slices: Y, A, 4 weights, rms, rms_total */
-                const double *src = &outs[n][s][0][0];
-                for (int e = 0; e < 256; e++) dst[s * 256 + e] = src[e];
-            }
-        }
-        done++;
-    }
-    if (texture_rbg && texture_rbg_stride) {
-        const size_t slice_stride = texture_rbg_stride * (size_t)(woi[3] + 1) * 8;
-        for (int n = 0; n < num_texture_tiles; n++) {
+        for (int n = n0; n < n1; n++) {
             int code = texture_indices[n];
-            if (!(code & (1 << 7))) continue;
             int tile = code >> 8;
-            if (tile < 0 || tile >= ntiles) continue;
+            valid[n - n0] = (code & (1 << 7)) && tile >= 0 && tile < ntiles;
+            if (!valid[n - n0]) continue;
+            texture_tile(tile, clt, colors, lpf, min_shot, scale_shot, port_offsets, diff_sigma, chw,
+                         dust_remove, keep_weights, outs[n - n0], margin ? margin + (size_t)n * 256 : NULL);
+            if (texture_tiles && texture_stride) {
+                double *dst = texture_tiles + (size_t)n * texture_stride;
+                for (int s = 0; s < nslices_tile; s++) {
+                    /* colors==1 slices: Y, A, 4 weights, rms, rms_total */
+                    const double *src = &outs[n - n0][s][0][0];
+                    for (int e = 0; e < 256; e++) dst[s * 256 + e] = src[e];
+                }
+            }
+            done++;
+        }
+        if (!(texture_rbg && texture_rbg_stride)) continue;
+        for (int n = n0; n < n1; n++) {
+            if (!valid[n - n0]) continue;
+            int code = texture_indices[n];
+            int tile = code >> 8;
             int nbr = code & 0xf;
             if (!nbr) continue;
             int tyy = tile / TX, txx = tile - tyy * TX;
@@ -704,7 +706,7 @@ int tpo_textures_accumulate(const tp_geometry *g, const int *woi, const double *
             for (int s = 0; s < nslices_img; s++)
                 for (int r = 0; r < 16; r++)
                     for (int c = 0; c < 16; c++) {
-                        double v = outs[n][s][r][c];
+                        double v = outs[n - n0][s][r][c];
                         if (nbr != 0xf) v *= AFADE[nbr][r * 16 + c];
                         long gy = y0 + r, gx = x0 + c;
                         if (gy < 0 || gx < 0) continue;

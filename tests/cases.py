@@ -30,7 +30,7 @@ def rms_err(a, b):
 class Case:
     def __init__(self, width=256, height=256, seed=0, border_mode=0, pad_rows=16, pitch_extra=64,
                  kernels="gauss", zero_extra=False, jitter=0.5, scene=None, mask=None,
-                 task_bits=synth.ALL_TASK_BITS, debug_marks=0):
+                 task_bits=synth.ALL_TASK_BITS, debug_marks=0, peak=1.0):
         self.seed = seed
         rng = np.random.default_rng(seed)
         self.geom = synth.geometry(width, height, border_mode=border_mode, image_rows=height + pad_rows,
@@ -41,7 +41,7 @@ class Case:
         self.rows = height + pad_rows
         disp = None
         if scene == "plane":
-            imgs, disp = synth.plane_scene(rng, width, height, disparity=(0.0, 16.0))
+            imgs, disp = synth.plane_scene(rng, width, height, disparity=(0.0, 16.0), peak=peak)
         else:
             imgs = synth.smooth_bayer(rng, width, height)
         self.images = imgs

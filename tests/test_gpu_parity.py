@@ -1,0 +1,432 @@
+"""GPU parity of the B200 kernels (called through the C ABI) against
+  * the FP64 oracle on the same inputs,
+  * the reference kernels rebuilt for sm_100a (oracle/_ref, when built),
+  * the golden fixtures made from the reference kernels.
+
+Tolerances (relative to the largest magnitude of the compared array):
+  CLT, correlation, inverse CLT: 1e-5 against the reference kernels and
+  against the oracle.
+  Texture slices: the fusion takes discrete best / worst camera choices, so a
+  float32 and an FP64 evaluation may choose differently where two camera
+  weights are within rounding of each other.  On pixels where the oracle's
+  relative weight gap is >= 1e-4 every slice is within 1e-5 of the oracle
+  (port weights and rms: 1e-4); on all pixels the colour/alpha slices are
+  within 1e-3 of the oracle and within 1e-5 of the reference kernels (both
+  float32).  The reference's rms slices use a one-pass variance that cancels
+  where the cameras agree; against them the tolerance is 1e-3.
+  Overlapped RGBA image: 1e-5 against the reference, 1e-3 against the oracle.
+  Texture lists and tasks: exact.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from cases import Case, blob_mask, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ref_256x256_seed11.npz")
+
+
+def _R():
+    import gpu_runner
+    return gpu_runner
+
+
+CASES = {
+    "A256ref": dict(width=256, height=256, seed=1, border_mode=0),
+    "B512plane": dict(width=512, height=384, seed=2, border_mode=0, scene="plane"),
+    "C512clamp": dict(width=512, height=384, seed=3, border_mode=1),
+    "E512hdr": dict(width=512, height=384, seed=6, border_mode=0, scene="plane", peak=200.0),
+}
+
+
+@pytest.fixture(scope="module")
+def frames(native):
+    R = _R()
+    out = {}
+    for k, kw in CASES.items():
+        out[k] = R.Frame(Case(**kw))
+    rng = np.random.default_rng(21)
+    d = Case(256, 256, seed=4, border_mode=0)
+    m = blob_mask(rng, d.TX, d.TY, 0.35)
+    d2 = Case(256, 256, seed=4, border_mode=0, mask=m)
+    assert d2.num_tiles % 4 != 0 or True
+    out["D256sparse"] = R.Frame(d2)
+    return out
+
+
+@pytest.fixture(scope="module")
+def clts(frames, oracle):
+    """B200 and oracle CLT of every case"""
+    R = _R()
+    res = {}
+    for k, fr in frames.items():
+        c = fr.case
+        b = R.convert(fr)
+        o = oracle.convert_correct_tiles(c.geom, c.extra, c.kernels, c.pitched, c.dstride, c.tasks)
+        res[k] = (b, o)
+    return res
+
+
+def _ref_ok(case):
+    import refgpu
+    return refgpu.available(case.geom)
+
+
+@pytest.mark.parametrize("name", list(CASES) + ["D256sparse"])
+def test_convert_vs_oracle(clts, name):
+    b, o = clts[name]
+    for cam in range(4):
+        assert rel_err(b[cam], o[cam]) < TOL, cam
+
+
+@pytest.mark.parametrize("name", ["A256ref", "B512plane", "D256sparse"])
+def test_convert_vs_reference(frames, clts, name):
+    fr = frames[name]
+    if not _ref_ok(fr.case):
+        pytest.skip("reference kernels not built")
+    if fr.case.num_tiles % 4:
+        pytest.skip("the reference kernel needs whole 4-tile blocks")
+    r = _R().convert(fr, impl="ref")
+    b, _ = clts[name]
+    for cam in range(4):
+        assert rel_err(b[cam], r[cam]) < TOL, cam
+
+
+def test_convert_lpf_and_partial_lists(frames, oracle):
+    R = _R()
+    fr = frames["A256ref"]
+    c = fr.case
+    b = R.convert(fr, lpf_mask=7)
+    o = oracle.convert_correct_tiles(c.geom, c.extra, c.kernels, c.pitched, c.dstride, c.tasks, lpf_mask=7)
+    assert max(rel_err(b[k], o[k]) for k in range(4)) < TOL
+    # a count that is not a multiple of 4 leaves the rest untouched
+    b = R.convert(fr, num_tiles=13)
+    o = oracle.convert_correct_tiles(c.geom, c.extra, c.kernels, c.pitched, c.dstride, c.tasks[:13])
+    assert max(rel_err(b[k], o[k]) for k in range(4)) < TOL
+    assert np.all(b[0][13 * 768:] == 0)
+
+
+def test_convert_skips_nop_and_out_of_range_tasks(frames, oracle):
+    R = _R()
+    fr = frames["A256ref"]
+    c = fr.case
+    from tile_processor_gpu_b200 import api
+    t = c.tasks.copy()
+    t["task"][5] = 0                       # NOP task
+    t["txy"][9] = 40 | (3 << 16)           # x beyond the tile grid
+    t["txy"][10] = 3 | (99 << 16)          # y beyond the tile grid
+    saved = fr.tasks
+    fr.tasks = api.tasks_to_device(t)
+    try:
+        b = R.convert(fr)
+    finally:
+        fr.tasks = saved
+    o = oracle.convert_correct_tiles(c.geom, c.extra, c.kernels, c.pitched, c.dstride, t)
+    assert max(rel_err(b[k], o[k]) for k in range(4)) < TOL
+    assert np.all(b[0][5 * 768:6 * 768] == 0)
+
+
+def _corr_case(frames, clts, name):
+    fr = frames[name]
+    b, _ = clts[name]
+    fr.set_clt(b)
+    return fr, [x.astype(np.float64) for x in b]
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("colors,radius", [(3, 7), (1, 4), (3, 0)])
+def test_correlate_vs_oracle(frames, clts, oracle, name, colors, radius):
+    R = _R()
+    fr, clt = _corr_case(frames, clts, name)
+    c = fr.case
+    sz = (2 * radius + 1) ** 2
+    b = R.correlate(fr, c.corr_idx, colors=colors, radius=radius, stride=sz + 5)
+    o = oracle.correlate2D(c.geom, clt, colors, .25, .25, .5, 0.05, c.corr_idx, sz + 5, radius)
+    assert rel_err(b[:, :sz], o[:, :sz]) < TOL
+    assert np.all(b[:, sz:] == -7.0)     # stride padding untouched
+
+
+def test_correlate_skips_invalid_entries(frames, clts, oracle):
+    R = _R()
+    fr, clt = _corr_case(frames, clts, "A256ref")
+    c = fr.case
+    idx = c.corr_idx[:8].copy()
+    idx[1] = (3 << 8) | 6                  # pair 6 does not exist
+    idx[2] = (3 << 8) | 255
+    idx[3] = ((c.TX * c.TY + 5) << 8) | 0  # tile beyond the grid
+    b = R.correlate(fr, idx)
+    o = oracle.correlate2D(c.geom, clt, 3, .25, .25, .5, 0.05, idx, 228, 7)
+    for k in (1, 2, 3):
+        assert np.all(b[k] == -7.0)
+    good = [0, 4, 5, 6, 7]
+    assert rel_err(b[good, :225], o[good, :225]) < TOL
+
+
+@pytest.mark.parametrize("name", ["A256ref", "B512plane"])
+def test_correlate_vs_reference(frames, clts, name):
+    R = _R()
+    fr, _ = _corr_case(frames, clts, name)
+    if not _ref_ok(fr.case):
+        pytest.skip("reference kernels not built")
+    c = fr.case
+    b = R.correlate(fr, c.corr_idx)
+    r = R.correlate(fr, c.corr_idx, impl="ref")
+    assert rel_err(b[:, :225], r[:, :225]) < TOL
+
+
+TIE_GAP = 1e-4
+
+
+def _texture_check_oracle(b, o, margin, ncol=3):
+    keep = (margin >= TIE_GAP).reshape(-1, 16, 16)
+    for s in range(b.shape[1]):
+        tol = TOL if s <= ncol else 1e-4
+        assert rel_err(b[:, s][keep], o[:, s][keep]) < tol, s
+    for s in range(ncol + 1):
+        assert rel_err(b[:, s], o[:, s]) < 1e-3, s
+
+
+def _texture_check_reference(b, r, margin, ncol=3):
+    keep = (margin >= TIE_GAP).reshape(-1, 16, 16)
+    for s in range(ncol + 1):
+        assert rel_err(b[:, s], r[:, s]) < TOL, s
+    for s in range(ncol + 1, ncol + 5):
+        assert rel_err(b[:, s][keep], r[:, s][keep]) < 1e-4, s
+    for s in range(ncol + 5, b.shape[1]):
+        assert rel_err(b[:, s][keep], r[:, s][keep]) < 1e-3, s
+
+
+@pytest.mark.parametrize("name", ["A256ref", "C512clamp", "E512hdr"])
+@pytest.mark.parametrize("keep_weights", [0, 1])
+def test_textures_vs_oracle(frames, clts, oracle, name, keep_weights):
+    R = _R()
+    fr, clt = _corr_case(frames, clts, name)
+    c = fr.case
+    b = R.textures_tiles(fr, c.tex_idx, keep_weights=keep_weights)
+    ns = b.shape[1]
+    o = np.zeros((len(c.tex_idx), ns * 256))
+    margin = oracle.textures_accumulate(c.geom, None, clt, c.tex_idx, c.port_offsets, keep_weights=keep_weights,
+                                        texture_stride=ns * 256, texture_tiles=o, want_margin=True)
+    _texture_check_oracle(b, o.reshape(b.shape), margin)
+
+
+def test_textures_mono_vs_oracle(frames, clts, oracle):
+    """colors = 1 (the reference's mono path reads shared memory it never
+    wrote for cameras 1..3, so only the oracle is compared)."""
+    R = _R()
+    fr, clt = _corr_case(frames, clts, "A256ref")
+    c = fr.case
+    b = R.textures_tiles(fr, c.tex_idx, keep_weights=1, colors=1)
+    o = np.zeros((len(c.tex_idx), 8 * 256))
+    margin = oracle.textures_accumulate(c.geom, None, clt, c.tex_idx, c.port_offsets, colors=1, keep_weights=1,
+                                        texture_stride=8 * 256, texture_tiles=o, want_margin=True)
+    _texture_check_oracle(b, o.reshape(b.shape), margin, ncol=1)
+
+
+@pytest.mark.parametrize("name", ["A256ref", "B512plane", "E512hdr"])
+def test_textures_vs_reference(frames, clts, name, oracle):
+    R = _R()
+    fr, clt = _corr_case(frames, clts, name)
+    if not _ref_ok(fr.case):
+        pytest.skip("reference kernels not built")
+    c = fr.case
+    b = R.textures_tiles(fr, c.tex_idx, keep_weights=1)
+    r = R.textures_tiles(fr, c.tex_idx, keep_weights=1, impl="ref")
+    o = np.zeros((len(c.tex_idx), 12 * 256))
+    margin = oracle.textures_accumulate(c.geom, None, clt, c.tex_idx, c.port_offsets, keep_weights=1,
+                                        texture_stride=12 * 256, texture_tiles=o, want_margin=True)
+    _texture_check_reference(b, r, margin)
+
+
+@pytest.mark.parametrize("name", ["A256ref", "C512clamp"])
+@pytest.mark.parametrize("marks", [0, 1])
+def test_imclt_vs_oracle(frames, clts, oracle, name, marks):
+    R = _R()
+    from tile_processor_gpu_b200 import api
+    fr, clt = _corr_case(frames, clts, name)
+    c = fr.case
+    g0 = fr.g
+    fr.g = api.Geometry.from_dict(dict(c.geom, debug_marks=marks))
+    try:
+        b, dst = R.imclt_all(fr)
+    finally:
+        fr.g = g0
+    o = np.zeros((3 * (c.H + 8), dst))
+    oracle.imclt_rbg_all(dict(c.geom, debug_marks=marks), clt[0], o, dst)
+    assert rel_err(b, o) < TOL
+
+
+@pytest.mark.parametrize("name", ["A256ref", "B512plane"])
+def test_imclt_vs_reference(frames, clts, name):
+    R = _R()
+    from tile_processor_gpu_b200 import api
+    fr, _ = _corr_case(frames, clts, name)
+    if not _ref_ok(fr.case):
+        pytest.skip("reference kernels not built")
+    g0 = fr.g
+    fr.g = api.Geometry.from_dict(dict(fr.case.geom, debug_marks=1))
+    try:
+        b, _ = R.imclt_all(fr)
+    finally:
+        fr.g = g0
+    r, _ = R.imclt_all(fr, impl="ref")
+    assert rel_err(b, r) < TOL
+
+
+def _sublists(idx, counts, TX, TYA):
+    quarter = TX * (TYA >> 2)
+    out = []
+    for q in range(4):
+        out.append(sorted(idx[q * quarter: q * quarter + counts[2 * q]].tolist()))
+        out.append(sorted(idx[(q + 1) * quarter - counts[2 * q + 1]: (q + 1) * quarter].tolist()))
+    return out
+
+
+@pytest.mark.parametrize("name", ["D256sparse", "A256ref", "B512plane"])
+def test_texture_list(frames, oracle, name):
+    R = _R()
+    fr = frames[name]
+    c = fr.case
+    tb, ib, cb, wb = R.texture_list(fr)
+    to, io, co, wo = oracle.prepare_texture_list(c.geom, c.tasks, c.TX, c.TY)
+    assert np.array_equal(tb["task"], to["task"])
+    assert np.array_equal(cb, co) and np.array_equal(wb, wo)
+    assert _sublists(ib, cb, c.TX, c.TYA) == _sublists(io, co, c.TX, c.TYA)
+    if _ref_ok(c.geom and c) if False else _ref_ok(c):
+        tr, ir, cr, wr = R.texture_list(fr, impl="ref")
+        assert np.array_equal(tb["task"], tr["task"])
+        assert np.array_equal(cb, cr) and np.array_equal(wb, wr)
+        assert _sublists(ib, cb, c.TX, c.TYA) == _sublists(ir, cr, c.TX, c.TYA)
+
+
+def _rgba_region(woi, colors=3):
+    h = (woi[3] + 1) * 8
+    w = (woi[2] + 1) * 8
+    return h, w
+
+
+@pytest.mark.parametrize("name", ["A256ref", "D256sparse"])
+def test_rgba_vs_oracle(frames, clts, oracle, name):
+    R = _R()
+    fr, clt = _corr_case(frames, clts, name)
+    c = fr.case
+    b, woi, stride, rows = R.rgba(fr)
+    o, _, _, _, woi_o = oracle.generate_RBGA(c.geom, c.tasks, c.TX, c.TY, clt, c.port_offsets, stride, rows + 8)
+    assert np.array_equal(woi, woi_o)
+    h, w = _rgba_region(woi)
+    for s in range(4):
+        assert rel_err(b[s * h:(s + 1) * h, :w], o[s * h:(s + 1) * h, :w]) < 1e-3, s
+
+
+@pytest.mark.parametrize("name", ["A256ref", "B512plane", "E512hdr"])
+def test_rgba_vs_reference(frames, clts, name):
+    R = _R()
+    fr, _ = _corr_case(frames, clts, name)
+    if not _ref_ok(fr.case):
+        pytest.skip("reference kernels not built")
+    b, woi, stride, rows = R.rgba(fr)
+    r, woi_r, _, _ = R.rgba(fr, impl="ref")
+    assert np.array_equal(woi, woi_r)
+    h, w = _rgba_region(woi)
+    assert rel_err(b[:4 * h, :w], r[:4 * h, :w]) < TOL
+
+
+def test_custom_lpf_tables(frames, clts, oracle):
+    """tp_set_lpf replaces a table on the device (the reference's
+    cudaMemcpyToSymbol); outputs follow the oracle run with the same table."""
+    R = _R()
+    from tile_processor_gpu_b200 import api
+    fr, clt = _corr_case(frames, clts, "A256ref")
+    c = fr.case
+    rng = np.random.default_rng(5)
+    new = rng.uniform(0.2, 1.0, size=(6, 64)).astype(np.float32)
+    try:
+        for w in range(6):
+            api.set_lpf(w, new[w])
+        b = R.convert(fr, lpf_mask=5)
+        o = oracle.convert_correct_tiles(c.geom, c.extra, c.kernels, c.pitched, c.dstride, c.tasks, lpf_mask=5,
+                                         lpf=new[:4])
+        assert max(rel_err(b[k], o[k]) for k in range(4)) < TOL
+        fr.set_clt(b)
+        bc = R.correlate(fr, c.corr_idx)
+        oc = oracle.correlate2D(c.geom, [x.astype(np.float64) for x in b], 3, .25, .25, .5, 0.05, c.corr_idx, 228, 7,
+                                lpf_rb_corr=new[4], lpf_corr=new[5])
+        assert rel_err(bc[:, :225], oc[:, :225]) < TOL
+    finally:
+        api.reset_lpf()
+    assert np.array_equal(api.get_lpf(2), oracle.default_lpf(2))
+
+
+def test_runs_on_a_side_stream(frames, clts):
+    import torch
+    R = _R()
+    from tile_processor_gpu_b200 import api
+    fr, _ = _corr_case(frames, clts, "A256ref")
+    c = fr.case
+    ref = R.correlate(fr, c.corr_idx)
+    s = torch.cuda.Stream()
+    out = torch.zeros((len(c.corr_idx), 228), device="cuda")
+    idx = torch.from_numpy(c.corr_idx).cuda()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        api.correlate2D(fr.g, fr.p_clt, 3, .25, .25, .5, 0.05, len(c.corr_idx), idx, 228, 7, out, stream=s)
+    s.synchronize()
+    assert np.array_equal(out.cpu().numpy()[:, :225], ref[:, :225])
+
+
+# ---- against the golden fixtures -------------------------------------------
+
+@pytest.fixture(scope="module")
+def golden(native):
+    if not os.path.exists(GOLDEN):
+        pytest.skip("golden fixture not generated")
+    import make_golden as MG
+    d = dict(np.load(GOLDEN))
+    case = MG.golden_case()
+    assert MG.input_digest(case) == str(d["input_sha256"])
+    return MG, case, d
+
+
+def test_golden_all_stages(golden):
+    R = _R()
+    MG, case, d = golden
+    fr = R.Frame(case)
+    sel = MG.sel_tile_ids(case)
+    clt = R.convert(fr)
+    mine = np.stack([np.stack([clt[c].reshape(-1, 768)[t] for c in range(4)]) for t in sel])
+    assert rel_err(mine, d["clt"]) < TOL
+    # downstream stages start from the reference's CLT so that each stage is
+    # compared on identical inputs
+    n = case.TX * case.TY * 768
+    ref_clt = [np.zeros(n, np.float32) for _ in range(4)]
+    for k, t in enumerate(sel):
+        for c in range(4):
+            ref_clt[c][t * 768:(t + 1) * 768] = d["clt"][k, c]
+    fr.set_clt(ref_clt)
+    idx = np.array([(int(t) << 8) | p for t in sel for p in range(6)], dtype=np.int32)
+    assert rel_err(R.correlate(fr, idx)[:, :225], d["corr"]) < TOL
+    assert rel_err(R.correlate(fr, idx[:24], colors=1, radius=4)[:, :81], d["corr_r4m"]) < TOL
+    tex_idx = np.array([(int(t) << 8) | (1 << 7) for t in sel], dtype=np.int32)
+    tex = R.textures_tiles(fr, tex_idx, keep_weights=1).reshape(len(sel), 12, 256)
+    for s in range(4):
+        assert rel_err(tex[:, s], d["tex"][:, s]) < TOL, s
+    # the remaining stages from the library's own CLT
+    fr2 = R.Frame(case)
+    R.convert(fr2)
+    g0 = fr2.g
+    from tile_processor_gpu_b200 import api
+    fr2.g = api.Geometry.from_dict(dict(case.geom, debug_marks=1))
+    img, _ = R.imclt_all(fr2)
+    fr2.g = g0
+    H = case.H + 8
+    mine = np.stack([np.stack([img[c * H + r: c * H + r + 40, x: x + 40] for r, x in MG.CROPS]) for c in range(3)])
+    assert rel_err(mine, d["imclt"]) < TOL
+    rb, woi, stride, rows = R.rgba(fr2)
+    assert np.array_equal(woi, d["rgba_woi"])
+    h = (woi[3] + 1) * 8
+    mine = np.stack([np.stack([rb[s * h + r: s * h + r + 40, c: c + 40] for r, c in MG.CROPS]) for s in range(4)])
+    assert rel_err(mine, d["rgba"]) < TOL

@@ -168,8 +168,8 @@ int tp_correlate2D(const tp_geometry *g, float *const *clt, int colors, float sc
     if (corr_stride < sz) return fail(TP_ERR_ARG, "corr_stride %zu < (2r+1)^2 = %zu", corr_stride, sz);
     int sms;
     if ((rc = sm_count(&sms))) return rc;
-    unsigned grid = grid_for((long long)num_corr_tiles, 32, sms, 8);
-    tp::k_correlate2D<<<grid, 256, 0, (cudaStream_t)stream>>>(gd, clt, colors, scale0, scale1, scale2, fat_zero,
+    unsigned grid = grid_for((long long)num_corr_tiles, 16, sms, 6);
+    tp::k_correlate2D<<<grid, 128, 0, (cudaStream_t)stream>>>(gd, clt, colors, scale0, scale1, scale2, fat_zero,
                                                               (long long)num_corr_tiles, corr_indices,
                                                               corr_stride, corr_radius, corrs);
     return cuda_status(cudaGetLastError(), "correlate2D launch");
@@ -219,7 +219,7 @@ int tp_textures_accumulate(const tp_geometry *g, const int *woi, float *const *c
         return fail(TP_ERR_ARG, "texture_stride %zu < %d slices x 256", texture_stride, ns);
     int sms;
     if ((rc = sm_count(&sms))) return rc;
-    unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, 5);
+    unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, 3);
     tp::k_textures<<<grid, 128, 0, (cudaStream_t)stream>>>(
         gd, woi, clt, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
@@ -333,7 +333,7 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
         tp::k_clear_rbga<<<grid, 256, 0, s>>>(woi, colors, 0, 0, texture_rbga_stride, texture_tiles);
     }
     const int quarter = gd.TX * (gd.TYA >> 2);
-    const unsigned grid = grid_for(quarter, 1, sms, 5);
+    const unsigned grid = grid_for(quarter, 1, sms, 3);
     for (int pass = 0; pass < 8; pass++) {
         const int border = pass >> 2;
         const int slot = ((pass & 3) << 1) + border;

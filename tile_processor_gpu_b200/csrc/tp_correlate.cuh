@@ -18,14 +18,18 @@
 
 namespace tp {
 
-__global__ void __launch_bounds__(256) k_correlate2D(Geom g, float *const *clt, int colors,
+/* per-group buffer: four 8x9 quadrants (transpose, then the pixel-domain
+ * quadrants), then the (2r+1)^2 output staging; 536 % 32 == 24 */
+constexpr int kCorrBuf = 4 * 72 + 8 + 240;
+
+__global__ void __launch_bounds__(128, 3) k_correlate2D(Geom g, float *const *clt, int colors,
                                                      float scale0, float scale1, float scale2,
                                                      float fat_zero, long long num_corr_tiles,
                                                      const int *__restrict__ corr_indices,
                                                      size_t corr_stride, int corr_radius,
                                                      float *__restrict__ corrs)
 {
-    __shared__ float tbuf[256 / 8][kTB4];
+    __shared__ float tbuf[128 / 8][kCorrBuf];
     const int l = threadIdx.x & 7;
     const int grp = threadIdx.x >> 3;
     const unsigned gm = group_mask();
@@ -33,6 +37,7 @@ __global__ void __launch_bounds__(256) k_correlate2D(Geom g, float *const *clt, 
     const int ntiles = g.TX * g.TY;
     const int r = corr_radius, sz = 2 * r + 1;
     float *tb = tbuf[grp];
+    float *stage = tb + 296;
     for (long long n = (long long)blockIdx.x * (blockDim.x >> 3) + grp; n < num_corr_tiles; n += groups_total) {
         const int code = corr_indices[n];
         const int tile = code >> 8, pair = code & 0xff;
@@ -82,8 +87,8 @@ __global__ void __launch_bounds__(256) k_correlate2D(Geom g, float *const *clt, 
             for (int q = 0; q < 4; q++) acc[q][m] = (acc[q][m] * sc) * f;
         }
         /* pixel domain: vertical DCT-II (q0,q1) / DST-II (q2,q3) on the held
-         * column, transpose, horizontal DCT-II (q0,q2) / DST-II (q1,q3) */
-        float pix[4][8];
+         * column, transpose, horizontal DCT-II (q0,q2) / DST-II (q1,q3); the
+         * result row l of quadrant q replaces its transpose buffer */
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             float v[8], row[8];
@@ -94,33 +99,23 @@ __global__ void __launch_bounds__(256) k_correlate2D(Geom g, float *const *clt, 
 #pragma unroll
             for (int k = 0; k < 8; k++) row[k] = tb[TBI(q, k, l)];
             __syncwarp(gm);
-            if (q & 1) dtt8<3>(row, pix[q]); else dtt8<2>(row, pix[q]);
-        }
-        /* unfold (lane i = row i): R[+-i][+-j] from q0[i][j], q1[i][j-1],
-         * q2[i-1][j], q3[i-1][j-1] */
-        float p2u[8], p3u[8];
+            if (q & 1) dtt8<3>(row, v); else dtt8<2>(row, v);
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            p2u[k] = __shfl_up_sync(gm, pix[2][k], 1, 8);
-            p3u[k] = __shfl_up_sync(gm, pix[3][k], 1, 8);
+            for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
         }
-        float *stage = tb; /* 296 floats >= 225 */
+        __syncwarp(gm);
+        /* unfold (lane i = rows +-i): R[+-i][+-j] from q0[i][j], q1[i][j-1],
+         * q2[i-1][j], q3[i-1][j-1], scaled by 1/4 */
         if (l <= r) {
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                if (j > r) break;
-                const float q0 = pix[0][j];
-                const float q1 = j > 0 ? pix[1][j - 1] : 0.0f;
-                const float q2 = l > 0 ? p2u[j] : 0.0f;
-                const float q3 = (l > 0 && j > 0) ? p3u[j - 1] : 0.0f;
-                const float pp = 0.25f * ((q0 + q1) + (q2 + q3));
-                const float pm = 0.25f * ((q0 - q1) + (q2 - q3));
-                const float mp = 0.25f * ((q0 + q1) - (q2 + q3));
-                const float mm = 0.25f * ((q0 - q1) - (q2 - q3));
-                stage[(r + l) * sz + (r + j)] = pp;
-                stage[(r + l) * sz + (r - j)] = pm;
-                stage[(r - l) * sz + (r + j)] = mp;
-                stage[(r - l) * sz + (r - j)] = mm;
+            for (int j = 0; j <= r; j++) {
+                const float q0 = tb[TBI(0, l, j)];
+                const float q1 = j > 0 ? tb[TBI(1, l, j - 1)] : 0.0f;
+                const float q2 = l > 0 ? tb[TBI(2, l - 1, j)] : 0.0f;
+                const float q3 = (l > 0 && j > 0) ? tb[TBI(3, l - 1, j - 1)] : 0.0f;
+                stage[(r + l) * sz + (r + j)] = 0.25f * ((q0 + q1) + (q2 + q3));
+                stage[(r + l) * sz + (r - j)] = 0.25f * ((q0 - q1) + (q2 - q3));
+                stage[(r - l) * sz + (r + j)] = 0.25f * ((q0 + q1) - (q2 + q3));
+                stage[(r - l) * sz + (r - j)] = 0.25f * ((q0 - q1) - (q2 - q3));
             }
         }
         __syncwarp(gm);

@@ -4,15 +4,19 @@
  * :3847-4017, debayer_shot / debayer :4019-4199 and tile_combine_rgba
  * :4202-4665).
  *
- * One 128-thread block per listed tile (grid-stride).  Stage 1: twelve 8-lane
- * groups, one per (camera, color), low-pass the CLT tile, invert it (vertical
- * DCT-IV/DST-IV on the held column, transpose, horizontal pass on the held
- * row) and unfold it into a windowed 16x16 tile in shared memory.  Stage 2:
- * every thread takes pixels of all twelve tiles for the un-window / 3x3
- * debayer / shot-noise square root / re-window chain.  Stage 3: one thread per
- * pixel fuses the four cameras.  Stage 4: the slices are written as
- * non-overlapping 16x16 tiles and/or faded by the neighbour mask and added into
- * the overlapped RGBA image.
+ * One 128-thread block per listed tile (grid-stride).  Per (camera, color)
+ * job one 8-lane group, working only with __syncwarp on its own buffers:
+ *   1. low-pass filter and invert the CLT tile (vertical DCT-IV/DST-IV on the
+ *      held column, transpose, horizontal pass on the held row) and unfold it
+ *      into the windowed 16x16 tile M;
+ *   2. un-window M, debayer the interior with the 3x3 stencil, apply the
+ *      shot-noise square root and re-window into D (lane l owns columns l and
+ *      l + 8).
+ * After one block barrier every thread fuses the four cameras at two pixels
+ * (stage 3), and the slices are written as non-overlapping 16x16 tiles and/or
+ * faded by the neighbour mask and added into the overlapped RGBA image
+ * (stage 4).  Per-job buffers are 280 floats apart (280 % 32 == 24) so the
+ * four groups of a warp never share a bank.
  */
 #pragma once
 #include "tp_common.cuh"
@@ -26,13 +30,17 @@ struct TextureParams {
     int dust_remove, keep_weights;
 };
 
+constexpr int kJob = 280;        /* floats per 16x17 job tile, padded */
+#define JT(r, c) ((r) * 17 + (c))
+
+__device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
+
 /* windowed inverse CLT of one job into a [16][17] tile (w * d, no accumulate).
  * Quadrant signs of the unfold (idct_signs, src/TileProcessor.cuh:399-420)
  * factor into a vertical and a horizontal sign vector. */
-__device__ __forceinline__ void imclt_job(const float *__restrict__ src, const float *lpf,
-                                          float *tb, float (*mout)[17], int l, unsigned gm)
+__device__ __forceinline__ void imclt_job(const float *__restrict__ src, const float *lpf, float *tb,
+                                          float *mout, int l, unsigned gm)
 {
-    float y[4][8];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         float col[8], v[8], row[8];
@@ -48,47 +56,210 @@ __device__ __forceinline__ void imclt_job(const float *__restrict__ src, const f
 #pragma unroll
         for (int k = 0; k < 8; k++) row[k] = tb[TBI(q, l, k)];
         __syncwarp(gm);
-        if (q & 1) dtt8<1>(row, y[q]); else dtt8<0>(row, y[q]);
+        if (q & 1) dtt8<1>(row, v); else dtt8<0>(row, v);
+        /* pixel-domain row l of quadrant q replaces its transpose buffer */
+#pragma unroll
+        for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
     }
-    /* output rows whose fold index is l */
-    const int ra = (l >= 4) ? l - 4 : 11 - l;
-    const int rb = (l >= 4) ? 11 - l : 12 + l;
-#pragma unroll
+    __syncwarp(gm);
+    /* unfold: output row r reads fold row RIND[r]; lane l writes columns l
+     * and l + 8 of every row */
+#pragma unroll 1
     for (int h = 0; h < 2; h++) {
-        const int r = h ? rb : ra;
-        const int rq = r >> 2;
-        const float svc = (rq == 0) ? 1.0f : -1.0f; /* cosine vertical */
-        const float svs = (rq == 3) ? -1.0f : 1.0f; /* sine vertical   */
-        const float wr = 0.5f * c_hwin[r];
+        const int c = l + 8 * h;
+        const int v = (c < 4) ? c + 4 : (c < 12) ? 11 - c : c - 12;
+        const int cq = c >> 2;
+        const float shc = (cq == 0) ? 1.0f : -1.0f; /* cosine horizontal */
+        const float shs = (cq == 3) ? -1.0f : 1.0f; /* sine horizontal   */
+        const float wc = 0.5f * c_hwin[c];
 #pragma unroll
-        for (int c = 0; c < 16; c++) {
-            const int v = (c < 4) ? c + 4 : (c < 12) ? 11 - c : c - 12;
-            const int cq = c >> 2;
-            const float shc = (cq == 0) ? 1.0f : -1.0f;
-            const float shs = (cq == 3) ? -1.0f : 1.0f;
-            const float d01 = (svc * shc) * y[0][v] + (svc * shs) * y[1][v];
-            const float d23 = (svs * shc) * y[2][v] + (svs * shs) * y[3][v];
-            const float w = wr * (0.5f * c_hwin[c]);
-            mout[r][c] = w * (d01 + d23);
+        for (int r = 0; r < 16; r++) {
+            const int u = (r < 4) ? r + 4 : (r < 12) ? 11 - r : r - 12;
+            const int rq = r >> 2;
+            const float svc = (rq == 0) ? 1.0f : -1.0f;
+            const float svs = (rq == 3) ? -1.0f : 1.0f;
+            const float d01 = (svc * shc) * tb[TBI(0, u, v)] + (svc * shs) * tb[TBI(1, u, v)];
+            const float d23 = (svs * shc) * tb[TBI(2, u, v)] + (svs * shs) * tb[TBI(3, u, v)];
+            const float w = (0.5f * c_hwin[r]) * wc;
+            mout[JT(r, c)] = w * (d01 + d23);
         }
     }
 }
 
-__device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
+/* un-window, 3x3 debayer (interior 14x14; border copied), shot-noise square
+ * root, re-window: M -> D through the scratch tile T.  Lane l: columns l and
+ * l + 8.  hsq = sin^2 of the window, hsqi = its reciprocal. */
+__device__ __forceinline__ void debayer_job(const float *m, float *t, float *d, int rb_mode, float min_shot,
+                                            float scale_shot, const float *hsq, const float *hsqi, int l,
+                                            unsigned gm)
+{
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int c = l + 8 * h;
+        const float wx = hsqi[sym8(c)];
+#pragma unroll
+        for (int r = 0; r < 16; r++) t[JT(r, c)] = (m[JT(r, c)] * wx) * hsqi[sym8(r)];
+    }
+    __syncwarp(gm);
+    const float kshot = rsqrtf(min_shot);
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+        const int c = l + 8 * h;
+        const float wx = hsq[sym8(c)];
+        const bool cborder = (c == 0) || (c == 15);
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            float v;
+            if (cborder || r == 0 || r == 15) {
+                v = t[JT(r, c)];
+            } else {
+                const float orth = ((t[JT(r - 1, c)] + t[JT(r + 1, c)]) + t[JT(r, c - 1)]) + t[JT(r, c + 1)];
+                if (rb_mode) {
+                    const float diag = ((t[JT(r - 1, c - 1)] + t[JT(r - 1, c + 1)]) + t[JT(r + 1, c - 1)]) +
+                                       t[JT(r + 1, c + 1)];
+                    v = __fmaf_rn(0.0625f, diag, __fmaf_rn(0.125f, orth, 0.25f * t[JT(r, c)]));
+                } else {
+                    v = __fmaf_rn(0.125f, orth, 0.5f * t[JT(r, c)]);
+                }
+            }
+            if (scale_shot > 0.0f) v = scale_shot * ((v > min_shot) ? sqrtf(v) : (kshot * v));
+            d[JT(r, c)] = v * (wx * hsq[sym8(r)]);
+        }
+    }
+    __syncwarp(gm);
+}
 
-__global__ void __launch_bounds__(128) k_textures(
+/* Fuse the four cameras at one pixel (tile_combine_rgba, one pixel).
+ * D: debayered, M: plain tiles, both [job = cam * colors + color].
+ * Writes colors, alpha, 4 port weights and (keep_weights) colors+1 rms. */
+template <int COLORS>
+__device__ __forceinline__ void combine_pixel(const float *sd, const float *sm, float *out, int r, int c,
+                                              const float *pd2r, float ksigma, const float *chw, float wnd2,
+                                              int dust_remove, int keep_weights)
+{
+    const int e = JT(r, c);
+    float D[4][COLORS];
+#pragma unroll
+    for (int cam = 0; cam < 4; cam++)
+#pragma unroll
+        for (int col = 0; col < COLORS; col++) D[cam][col] = sd[(cam * COLORS + col) * kJob + e];
+    if (keep_weights) {
+        float sw = 0.0f;
+#pragma unroll
+        for (int col = 0; col < COLORS; col++) {
+            /* variance of the four cameras, two-pass (the one-pass form of
+             * the reference loses digits where the cameras agree) */
+            const float mean = ((D[0][col] + D[1][col]) + (D[2][col] + D[3][col])) * 0.25f;
+            float ss = 0.0f;
+#pragma unroll
+            for (int cam = 0; cam < 4; cam++) {
+                const float dv = D[cam][col] - mean;
+                ss = __fmaf_rn(dv, dv, ss);
+            }
+            const float mse = ss * 0.25f;
+            out[(COLORS + 5 + col) * kJob + e] = sqrtf(mse);
+            sw = __fmaf_rn(chw[col], mse, sw);
+        }
+        out[(COLORS + 5 + COLORS) * kJob + e] = sqrtf(sw);
+    }
+    const float wi = (float)(1.0 / (double)wnd2);
+    float pw[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    {
+        int k = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = i + 1; j < 4; j++) {
+                float d = 0.0f;
+#pragma unroll
+                for (int col = 0; col < COLORS; col++) {
+                    const float dc = (D[i][col] - D[j][col]) * wi;
+                    d = __fmaf_rn(chw[col] * dc, dc, d);
+                }
+                const float x = (float)((double)expf(-pd2r[k] * d) + 0.0001);
+                pw[i] += x;
+                pw[j] += x;
+                k++;
+            }
+    }
+    int b1 = 0;
+#pragma unroll
+    for (int cam = 1; cam < 4; cam++) if (pw[cam] > pw[b1]) b1 = cam;
+    int b2 = (b1 == 0) ? 1 : 0;
+#pragma unroll
+    for (int cam = 1; cam < 4; cam++) if (cam > b2 && cam != b1 && pw[cam] > pw[b2]) b2 = cam;
+    float p1 = 0.0f, p2 = 0.0f;
+#pragma unroll
+    for (int cam = 0; cam < 4; cam++) {
+        if (cam == b1) p1 = pw[cam];
+        if (cam == b2) p2 = pw[cam];
+    }
+    const float w1 = p1 / (p1 + p2);
+    const float w2 = 1.0f - w1;
+    float avg[COLORS];
+#pragma unroll
+    for (int col = 0; col < COLORS; col++) {
+        float a = 0.0f, b = 0.0f;
+#pragma unroll
+        for (int cam = 0; cam < 4; cam++) {
+            if (cam == b1) a = D[cam][col];
+            if (cam == b2) b = D[cam][col];
+        }
+        avg[col] = w1 * a + w2 * b;
+    }
+#pragma unroll
+    for (int cam = 0; cam < 4; cam++) {
+        float d2 = 0.0f;
+#pragma unroll
+        for (int col = 0; col < COLORS; col++) {
+            const float dc = (D[cam][col] - avg[col]) * wi;
+            d2 = __fmaf_rn(chw[col] * dc, dc, d2);
+        }
+        pw[cam] = (float)((double)expf(-ksigma * d2) + 0.0001);
+    }
+    if (dust_remove) {
+        int worst = 0;
+#pragma unroll
+        for (int cam = 1; cam < 4; cam++) if (pw[cam] < pw[worst]) worst = cam;
+        float wv = 0.0f;
+#pragma unroll
+        for (int cam = 0; cam < 4; cam++) if (cam == worst) wv = pw[cam];
+        float a = -wv;
+#pragma unroll
+        for (int cam = 0; cam < 4; cam++) a += pw[cam];
+        a /= 3.0f;
+        const float scale = (float)(1.0 + (double)(wv * (a - wv) / (a * a * 3.0f)));
+        const float fw = wv / a;
+#pragma unroll
+        for (int cam = 0; cam < 4; cam++) pw[cam] *= (cam == worst) ? fw : scale;
+    }
+    float ksum = 0.0f;
+#pragma unroll
+    for (int cam = 0; cam < 4; cam++) ksum += pw[cam];
+    const float kinv = (float)(1.0 / (double)ksum);
+#pragma unroll
+    for (int col = 0; col < COLORS; col++) {
+        float v = 0.0f;
+#pragma unroll
+        for (int cam = 0; cam < 4; cam++) v = __fmaf_rn(kinv * pw[cam], sm[(cam * COLORS + col) * kJob + e], v);
+        out[col * kJob + e] = v;
+    }
+    out[COLORS * kJob + e] = wnd2 * ksum / 4.0f;
+#pragma unroll
+    for (int cam = 0; cam < 4; cam++) out[(COLORS + 1 + cam) * kJob + e] = pw[cam];
+}
+
+__global__ void __launch_bounds__(128, 3) k_textures(
     Geom g, const int *__restrict__ woi, float *const *clt, long long num_texture_tiles,
     const int *__restrict__ list, const int *__restrict__ dev_counts, int count_slot, int list_cap,
     int border_quarter, const float *__restrict__ port_offsets, TextureParams p,
     size_t texture_rbg_stride, float *__restrict__ texture_rbg, size_t texture_stride,
     float *__restrict__ texture_tiles)
 {
-    __shared__ float s_m[12][16][17];      /* IMCLT tiles (not debayered)  */
-    __shared__ float s_t[12][16][17];      /* un-windowed; later the slices */
-    __shared__ union {
-        float tb[12][kTB4];                /* stage-1 transposes           */
-        float d[12][16][17];               /* debayered tiles              */
-    } s_u;
+    __shared__ float s_m[12 * kJob];   /* IMCLT tiles (not debayered)              */
+    __shared__ float s_d[12 * kJob];   /* debayered tiles                          */
+    __shared__ float s_x[12 * kTB4];   /* transposes, then un-windowed tiles, then
+                                        * the output slices (12 x kJob floats)     */
     __shared__ float s_hsq[16], s_hsqi[16];
 
     const int tid = threadIdx.x;
@@ -134,156 +305,34 @@ __global__ void __launch_bounds__(128) k_textures(
         const int tile = code >> 8;
         if (!(code & (1 << 7)) || tile < 0 || tile >= g.TX * g.TY) continue;
 
-        /* ---- stage 1: LPF + inverse CLT per (camera, color) ---- */
+        /* ---- stages 1-2: per (camera, color) group ---- */
         if (grp < njobs) {
             const int cam = grp / colors, color = grp - cam * colors;
             const float *src = clt[cam] + ((size_t)tile * 3 + color) * 256;
-            imclt_job(src, c_lpf[colors > 1 ? color : 3], s_u.tb[grp], s_m[grp], l, gm);
-        }
-        __syncthreads();
-
-        /* ---- stage 2: debayer with shot-noise correction ---- */
-        if (colors > 1) {
-            for (int e = tid; e < 12 * 256; e += 128) {
-                const int j = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                s_t[j][r][c] = (s_m[j][r][c] * s_hsqi[sym8(c)]) * s_hsqi[sym8(r)];
-            }
-            __syncthreads();
-            const float kshot = rsqrtf(p.min_shot);
-            for (int e = tid; e < 12 * 256; e += 128) {
-                const int j = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                const int color = j % 3;
-                float v;
-                if (r == 0 || r == 15 || c == 0 || c == 15) {
-                    v = s_t[j][r][c];
-                } else {
-                    const float orth = ((s_t[j][r - 1][c] + s_t[j][r + 1][c]) + s_t[j][r][c - 1]) + s_t[j][r][c + 1];
-                    if (color < 2) {
-                        const float diag = ((s_t[j][r - 1][c - 1] + s_t[j][r - 1][c + 1]) + s_t[j][r + 1][c - 1]) + s_t[j][r + 1][c + 1];
-                        v = (float)(0.0625 * (double)diag + 0.125 * (double)orth + 0.25 * (double)s_t[j][r][c]);
-                    } else {
-                        v = (float)(0.125 * (double)orth + 0.5 * (double)s_t[j][r][c]);
-                    }
+            float *mj = s_m + grp * kJob, *dj = s_d + grp * kJob, *xj = s_x + grp * kTB4;
+            imclt_job(src, c_lpf[colors > 1 ? color : 3], xj, mj, l, gm);
+            __syncwarp(gm);
+            if (colors > 1) {
+                debayer_job(mj, xj, dj, color < 2, p.min_shot, p.scale_shot, s_hsq, s_hsqi, l, gm);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 16; r++) {
+                    dj[JT(r, l)] = mj[JT(r, l)];
+                    dj[JT(r, l + 8)] = mj[JT(r, l + 8)];
                 }
-                if (p.scale_shot > 0.0f) v = p.scale_shot * ((v > p.min_shot) ? sqrtf(v) : (kshot * v));
-                s_u.d[j][r][c] = v * (s_hsq[sym8(c)] * s_hsq[sym8(r)]);
-            }
-        } else {
-            for (int e = tid; e < 4 * 256; e += 128) {
-                const int j = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                s_u.d[j][r][c] = s_m[j][r][c];
             }
         }
         __syncthreads();
 
         /* ---- stage 3: fuse the four cameras, one thread per pixel ---- */
-        float(*out)[16][17] = s_t; /* 12 slices */
+#pragma unroll 1
         for (int px = tid; px < 256; px += 128) {
             const int r = px >> 4, c = px & 15;
-            float D[4][3], M[4][3];
-#pragma unroll
-            for (int cam = 0; cam < 4; cam++)
-#pragma unroll
-                for (int col = 0; col < 3; col++) {
-                    if (col < colors) {
-                        D[cam][col] = s_u.d[cam * colors + col][r][c];
-                        M[cam][col] = s_m[cam * colors + col][r][c];
-                    } else {
-                        D[cam][col] = 0.0f;
-                        M[cam][col] = 0.0f;
-                    }
-                }
-            if (p.keep_weights) {
-                float sw = 0.0f;
-#pragma unroll
-                for (int col = 0; col < 3; col++) {
-                    if (col >= colors) break;
-                    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
-#pragma unroll
-                    for (int cam = 0; cam < 4; cam++) {
-                        s0 += 1.0f;
-                        s1 += D[cam][col];
-                        s2 = __fmaf_rn(D[cam][col], D[cam][col], s2);
-                    }
-                    const float mse = (s0 * s2 - s1 * s1) / (s0 * s0);
-                    out[colors + 5 + col][r][c] = sqrtf(mse);
-                    sw = __fmaf_rn(chw[col], mse, sw);
-                }
-                out[colors + 5 + colors][r][c] = sqrtf(sw);
-            }
             const float wnd2 = s_hsq[sym8(r)] * s_hsq[sym8(c)];
-            const float wi = (float)(1.0 / (double)wnd2);
-            float pw[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            {
-                int k = 0;
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-#pragma unroll
-                    for (int j = i + 1; j < 4; j++) {
-                        float d = 0.0f;
-#pragma unroll
-                        for (int col = 0; col < 3; col++) {
-                            if (col >= colors) break;
-                            const float dc = (D[i][col] - D[j][col]) * wi;
-                            d = __fmaf_rn(chw[col] * dc, dc, d);
-                        }
-                        const float e = (float)((double)expf(-pd2r[k] * d) + 0.0001);
-                        pw[i] += e;
-                        pw[j] += e;
-                        k++;
-                    }
-            }
-            int b1 = 0;
-#pragma unroll
-            for (int cam = 1; cam < 4; cam++) if (pw[cam] > pw[b1]) b1 = cam;
-            int b2 = (b1 == 0) ? 1 : 0;
-#pragma unroll
-            for (int cam = 1; cam < 4; cam++) if (cam > b2 && cam != b1 && pw[cam] > pw[b2]) b2 = cam;
-            const float w1 = pw[b1] / (pw[b1] + pw[b2]);
-            const float w2 = 1.0f - w1;
-            float avg[3];
-#pragma unroll
-            for (int col = 0; col < 3; col++) avg[col] = w1 * D[b1][col] + w2 * D[b2][col];
-#pragma unroll
-            for (int cam = 0; cam < 4; cam++) {
-                float d2 = 0.0f;
-#pragma unroll
-                for (int col = 0; col < 3; col++) {
-                    if (col >= colors) break;
-                    const float dc = (D[cam][col] - avg[col]) * wi;
-                    d2 = __fmaf_rn(chw[col] * dc, dc, d2);
-                }
-                pw[cam] = (float)((double)expf(-ksigma * d2) + 0.0001);
-            }
-            if (p.dust_remove) {
-                int worst = 0;
-#pragma unroll
-                for (int cam = 1; cam < 4; cam++) if (pw[cam] < pw[worst]) worst = cam;
-                const float wv = pw[worst];
-                float a = -wv;
-#pragma unroll
-                for (int cam = 0; cam < 4; cam++) a += pw[cam];
-                a /= 3.0f;
-                const float scale = (float)(1.0 + (double)(wv * (a - wv) / (a * a * 3.0f)));
-#pragma unroll
-                for (int cam = 0; cam < 4; cam++) if (cam != worst) pw[cam] *= scale;
-                pw[worst] *= wv / a;
-            }
-            float ksum = 0.0f;
-#pragma unroll
-            for (int cam = 0; cam < 4; cam++) ksum += pw[cam];
-            const float kinv = (float)(1.0 / (double)ksum);
-#pragma unroll
-            for (int col = 0; col < 3; col++) {
-                if (col >= colors) break;
-                float v = 0.0f;
-#pragma unroll
-                for (int cam = 0; cam < 4; cam++) v = __fmaf_rn(kinv * pw[cam], M[cam][col], v);
-                out[col][r][c] = v;
-            }
-            out[colors][r][c] = wnd2 * ksum / 4.0f;
-#pragma unroll
-            for (int cam = 0; cam < 4; cam++) out[colors + 1 + cam][r][c] = pw[cam];
+            if (colors == 3)
+                combine_pixel<3>(s_d, s_m, s_x, r, c, pd2r, ksigma, chw, wnd2, p.dust_remove, p.keep_weights);
+            else
+                combine_pixel<1>(s_d, s_m, s_x, r, c, pd2r, ksigma, chw, wnd2, p.dust_remove, p.keep_weights);
         }
         __syncthreads();
 
@@ -293,7 +342,7 @@ __global__ void __launch_bounds__(128) k_textures(
             float *dst = texture_tiles + (size_t)n * texture_stride;
             for (int e = tid; e < ns * 256; e += 128) {
                 const int s = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                dst[e] = out[s][r][c];
+                dst[e] = s_x[s * kJob + JT(r, c)];
             }
         }
         const int nbr = code & TP_TASK_TEXTURE_BITS;
@@ -302,7 +351,7 @@ __global__ void __launch_bounds__(128) k_textures(
             const long long x0 = (long long)(tx - wx0) * 8, y0 = (long long)(ty - wy0) * 8;
             for (int e = tid; e < (colors + 1) * 256; e += 128) {
                 const int s = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                float v = out[s][r][c];
+                float v = s_x[s * kJob + JT(r, c)];
                 if (nbr != TP_TASK_TEXTURE_BITS) v *= c_alpha_fade[nbr][r * 16 + c];
                 const long long gy = y0 + r, gx = x0 + c;
                 if (gy < 0 || gx < 0) continue;
