@@ -50,6 +50,10 @@ def _parr(arrs):
     return ptrs
 
 
+def set_table_mode(mode):
+    lib().tpo_set_table_mode(int(mode))
+
+
 def set_threads(n):
     lib().tpo_set_threads(int(n))
 

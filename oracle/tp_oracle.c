@@ -32,6 +32,11 @@
 
 static double DCT4[8][8], DST4[8][8], DCT2[8][8], DST2[8][8];
 static double HWIN[16];   /* sin(pi*(2n+1)/32): the 16-tap lapped window       */
+/* window tables as used by each stage; mode 1 rounds them to 6 decimals as
+ * the reference's printed tables are (HWINDOW, HWINDOW2, HWINDOW_SQ,
+ * HWINDOW_SQi, src/TileProcessor.cuh:374-383) */
+static double TW[16], TW2[16], TWSQ[16], TWSQI[16];
+static int table_mode = 0;
 static double AFADE[16][256];
 static int    RIND[16];   /* window sample n -> DTT index (fold and unfold)    */
 static int    tables_ready = 0;
@@ -61,7 +66,28 @@ static void init_tables(void)
         RIND[n] = (n < 4) ? n + 4 : (n < 12) ? 11 - n : n - 12;
     }
     tpo_alpha_fade(AFADE);
+    for (int n = 0; n < 16; n++) {
+        double v = HWIN[n];
+        if (table_mode == 1) {
+            TW[n] = nearbyint(v * 1e6) / 1e6;
+            TW2[n] = nearbyint(0.5 * v * 1e6) / 1e6;
+            TWSQ[n] = nearbyint(v * v * 1e6) / 1e6;
+            TWSQI[n] = nearbyint(1e6 / (v * v)) / 1e6;
+        } else {
+            TW[n] = v;
+            TW2[n] = 0.5 * v;
+            TWSQ[n] = v * v;
+            TWSQI[n] = 1.0 / (v * v);
+        }
+    }
     tables_ready = 1;
+}
+
+void tpo_set_table_mode(int mode)
+{
+    table_mode = mode ? 1 : 0;
+    tables_ready = 0;
+    init_tables();
 }
 
 void tpo_dtt_matrix(int kind, double out[64])
@@ -239,9 +265,13 @@ static void convert_one(const tp_geometry *g, const float *extra_tab, const floa
     /* shifted windows with the fold signs embedded (:3196-3262):
      * cos branch +,+,+,+,-,...,-; sine branch (green) +x12, -x4 */
     double whc[16], whs[16], wv[16];
+    const double ah = M_PI * (double)shx / 16.0, av = M_PI * (double)shy / 16.0;
     for (int n = 0; n < 16; n++) {
-        double sh = sin(M_PI * (2.0 * (n + (double)shx) + 1.0) / 32.0);
-        double sv = sin(M_PI * (2.0 * (n + (double)shy) + 1.0) / 32.0);
+        /* w(n + s) = w(n) cos(pi s / 16) + w'(n) sin(pi s / 16), w' the
+         * quadrature window (table mode 1 uses the 6-decimal w) */
+        double wq = (n < 8) ? TW[7 - n] : -TW[n - 8];
+        double sh = TW[n] * cos(ah) + wq * sin(ah);
+        double sv = TW[n] * cos(av) + wq * sin(av);
         whc[n] = (n < 4) ? sh : -sh;
         whs[n] = (n < 12) ? sh : -sh;
         wv[n]  = (n < 4) ? sv : -sv;
@@ -449,7 +479,7 @@ static void imclt_tile(const double q[4][8][8], double out[16][16])
             int a = rr >> 2, b = cc >> 2, u = RIND[rr], v = RIND[cc];
             double d = SGN_C[a] * SGN_C[b] * x[0][u][v] + SGN_C[a] * SGN_S[b] * x[1][u][v] +
                        SGN_S[a] * SGN_C[b] * x[2][u][v] + SGN_S[a] * SGN_S[b] * x[3][u][v];
-            out[rr][cc] = 0.25 * HWIN[rr] * HWIN[cc] * d;
+            out[rr][cc] = TW2[rr] * TW2[cc] * d;
         }
 }
 
@@ -497,7 +527,7 @@ static void debayer_shot(int rb_mode, double min_shot, double scale_shot,
 {
     double t[16][16];
     for (int r = 0; r < 16; r++)      /* remove the squared window (:4028-4044) */
-        for (int c = 0; c < 16; c++) t[r][c] = src[r][c] / (HWIN[r] * HWIN[r] * HWIN[c] * HWIN[c]);
+        for (int c = 0; c < 16; c++) t[r][c] = src[r][c] * TWSQI[r] * TWSQI[c];
     for (int r = 0; r < 16; r++)      /* 3x3 debayer of the interior (:4146-4199) */
         for (int c = 0; c < 16; c++) {
             if (r == 0 || r == 15 || c == 0 || c == 15) { dst[r][c] = t[r][c]; continue; }
@@ -518,7 +548,7 @@ static void debayer_shot(int rb_mode, double min_shot, double scale_shot,
             }
     }
     for (int r = 0; r < 16; r++)      /* re-apply the squared window */
-        for (int c = 0; c < 16; c++) dst[r][c] *= HWIN[r] * HWIN[r] * HWIN[c] * HWIN[c];
+        for (int c = 0; c < 16; c++) dst[r][c] *= TWSQ[r] * TWSQ[c];
 }
 
 static double rel_gap(double a, double b)
@@ -563,16 +593,20 @@ static void combine_rgba(int colors, const double D[4][3][16][16], const double 
                 }
                 crms[colors][r][c] = sqrt(sw);
             }
-            double wnd2 = HWIN[r] * HWIN[r] * HWIN[c] * HWIN[c];
+            double wnd2 = TWSQ[r] * TWSQ[c];
             double wi = 1.0 / wnd2;
-            double w[4] = {0, 0, 0, 0};
+            /* Camera weights are float32 in the reference (the exponential
+             * underflows to the 1e-4 floor, making weights exactly equal);
+             * they are kept in float here so the best / worst camera choices
+             * are the reference's.  Everything else stays FP64. */
+            float w[4] = {0, 0, 0, 0};
             for (int p = 0; p < 6; p++) {
                 double d = 0.0;
                 for (int col = 0; col < colors; col++) {
                     double dc = (D[pp[p][0]][col][r][c] - D[pp[p][1]][col][r][c]) * wi;
                     d += chw[col] * dc * dc;
                 }
-                double e = exp(-pd2r[p] * d) + 1e-4;
+                float e = (float)(exp(-pd2r[p] * d) + 1e-4);
                 w[pp[p][0]] += e;
                 w[pp[p][1]] += e;
             }
@@ -584,7 +618,7 @@ static void combine_rgba(int colors, const double D[4][3][16][16], const double 
                 if (cam != b1) gap = fmin(gap, rel_gap(w[b1], w[cam]));
                 if (cam != b1 && cam != b2) gap = fmin(gap, rel_gap(w[b2], w[cam]));
             }
-            double w1 = w[b1] / (w[b1] + w[b2]), w2 = 1.0 - w1;
+            double w1 = (double)w[b1] / ((double)w[b1] + (double)w[b2]), w2 = 1.0 - w1;
             double avg[3];
             for (int col = 0; col < colors; col++) avg[col] = w1 * D[b1][col][r][c] + w2 * D[b2][col][r][c];
             for (int cam = 0; cam < 4; cam++) {
@@ -593,29 +627,31 @@ static void combine_rgba(int colors, const double D[4][3][16][16], const double 
                     double dc = (D[cam][col][r][c] - avg[col]) * wi;
                     d2 += chw[col] * dc * dc;
                 }
-                w[cam] = exp(-ksigma * d2) + 1e-4;
+                w[cam] = (float)(exp(-ksigma * d2) + 1e-4);
             }
+            double wd[4];
+            for (int cam = 0; cam < 4; cam++) wd[cam] = w[cam];
             if (dust_remove) {
                 int worst = 0;
                 for (int cam = 1; cam < 4; cam++) if (w[cam] < w[worst]) worst = cam;
                 for (int cam = 0; cam < 4; cam++) if (cam != worst) gap = fmin(gap, rel_gap(w[worst], w[cam]));
-                double wv = w[worst];
+                double wv = wd[worst];
                 double a = -wv;
-                for (int cam = 0; cam < 4; cam++) a += w[cam];
+                for (int cam = 0; cam < 4; cam++) a += wd[cam];
                 a /= 3.0;
                 double scale = 1.0 + wv * (a - wv) / (a * a * 3.0);
-                for (int cam = 0; cam < 4; cam++) if (cam != worst) w[cam] *= scale;
-                w[worst] *= wv / a;
+                for (int cam = 0; cam < 4; cam++) if (cam != worst) wd[cam] *= scale;
+                wd[worst] *= wv / a;
             }
             double ws = 0.0;
-            for (int cam = 0; cam < 4; cam++) ws += w[cam];
+            for (int cam = 0; cam < 4; cam++) ws += wd[cam];
             for (int col = 0; col < colors; col++) {
                 double v = 0.0;
-                for (int cam = 0; cam < 4; cam++) v += (w[cam] / ws) * M[cam][col][r][c];
+                for (int cam = 0; cam < 4; cam++) v += (wd[cam] / ws) * M[cam][col][r][c];
                 rgba[col][r][c] = v;
             }
             alpha[r][c] = wnd2 * ws / 4.0;
-            for (int cam = 0; cam < 4; cam++) pw[cam][r][c] = w[cam];
+            for (int cam = 0; cam < 4; cam++) pw[cam][r][c] = wd[cam];
             if (margin) margin[r * 16 + c] = gap;
         }
 }

@@ -101,6 +101,10 @@ int tpo_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles,
                       size_t texture_rbga_rows,
                       const float *lpf);
 
+/* Window tables: 0 = exact (default), 1 = rounded to 6 decimals like the
+ * reference's printed tables (used to find outputs sensitive to them). */
+void tpo_set_table_mode(int mode);
+
 /* Worker threads used by the tile loops (OpenMP); 0 = all. */
 void tpo_set_threads(int n);
 int tpo_get_threads(void);

@@ -1,0 +1,69 @@
+"""Which texture outputs are well conditioned.
+
+The camera fusion of the texture stage (tile_combine_rgba) takes discrete
+choices -- best and second-best camera, worst camera for dust removal -- from
+weights that can be equal to within float32 rounding.  Near such a tie, any
+two correct implementations that round differently (the reference's
+butterflies with 6-digit constants, this library's matrix transforms, the
+FP64 oracle) may legitimately produce different outputs.
+
+A texture output is called *stable* when the FP64 oracle reproduces it to
+1e-5 (relative to the slice maximum) both after its input CLT is perturbed by
+random relative noise of 1e-6 -- about the size of the differences between
+float32 evaluations -- and when its window tables are rounded to 6 decimals
+as the reference's printed tables are (the 1/sin^4 edge weighting of the
+fusion amplifies that rounding, 3.8e-5 at the first tap).  The oracle keeps
+the camera weights in float32, as the reference does, so exact float ties
+resolve the same way.  Parity of texture outputs is checked, slice by slice,
+on stable outputs; the fraction of unstable ones is bounded.  On smooth
+scenes the colour and alpha slices are stable almost everywhere; the port
+weights of high-dynamic-range scenes, whose weights sit near the 1e-4 floor,
+are the ill-conditioned ones.
+"""
+import numpy as np
+
+EPS = 1e-6
+TOL = 1e-5
+
+
+def texture_outputs(oracle, case, clt64, idx, keep_weights=0, colors=3):
+    ns = (12 if keep_weights else 4) if colors == 3 else (8 if keep_weights else 2)
+    out = np.zeros((len(idx), ns * 256))
+    oracle.textures_accumulate(case.geom, None, clt64, idx, case.port_offsets, colors=colors,
+                               keep_weights=keep_weights, texture_stride=ns * 256, texture_tiles=out)
+    return out.reshape(len(idx), ns, 16, 16)
+
+
+def unstable_mask(oracle, case, clt64, idx, keep_weights=0, colors=3, trials=2, seed=100):
+    """(unstable [n][ns][16][16] bool per slice, oracle outputs [n][ns][16][16])"""
+    base = texture_outputs(oracle, case, clt64, idx, keep_weights, colors)
+    scale = np.maximum(np.abs(base).max(axis=(0, 2, 3)), 1e-300)[None, :, None, None]
+    bad = np.zeros(base.shape, dtype=bool)
+    for t in range(trials):
+        rng = np.random.default_rng(seed + t)
+        pert = [c * (1.0 + EPS * rng.standard_normal(c.shape)) for c in clt64]
+        o = texture_outputs(oracle, case, pert, idx, keep_weights, colors)
+        bad |= np.abs(o - base) / scale > TOL
+    oracle.set_table_mode(1)
+    try:
+        o = texture_outputs(oracle, case, clt64, idx, keep_weights, colors)
+    finally:
+        oracle.set_table_mode(0)
+    bad |= np.abs(o - base) / scale > TOL
+    return bad, base
+
+
+def unstable_image_mask(bad_tiles, idx, woi, TX, shape, slices):
+    """Map unstable tile pixels ([n][16][16], any slice) of the listed tiles
+    into the overlapped RGBA image ([slices * h][w]); shape = (h, w) of one
+    slice."""
+    h, w = shape
+    m = np.zeros((h, w), dtype=bool)
+    for k, code in enumerate(idx):
+        tile = int(code) >> 8
+        ty, tx = divmod(tile, TX)
+        y0, x0 = (ty - woi[1]) * 8, (tx - woi[0]) * 8
+        if y0 < 0 or x0 < 0:
+            continue
+        m[y0:y0 + 16, x0:x0 + 16] |= bad_tiles[k]
+    return np.concatenate([m] * slices, axis=0)

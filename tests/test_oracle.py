@@ -217,28 +217,22 @@ def test_golden_correlate(oracle, golden):
 
 
 def test_golden_textures(oracle, golden):
+    import conditioning
     MG, case, d = golden
     clt = _golden_clt_arrays(MG, case, d)
     sel = MG.sel_tile_ids(case)
     tex_idx = np.array([(int(t) << 8) | (1 << 7) for t in sel], dtype=np.int32)
-    out = np.zeros((len(sel), 12 * 256))
-    margin = oracle.textures_accumulate(case.geom, None, clt, tex_idx, case.port_offsets, keep_weights=1,
-                                        texture_stride=12 * 256, texture_tiles=out, want_margin=True)
-    out = out.reshape(len(sel), 12, 256)
-    ref = d["tex"]
-    # colour and alpha slices, away from near-tie camera choices
-    keep = margin >= 1e-4
+    bad, out = conditioning.unstable_mask(oracle, case, clt, tex_idx, keep_weights=1)
+    keep = ~bad
+    ref = d["tex"].reshape(out.shape)
     for s in range(4):
-        assert rel_err(out[:, s][keep], ref[:, s][keep]) < 1e-5, s
-        assert rel_err(out[:, s], ref[:, s]) < 1e-3, s
-    # port weights and rms follow discrete best/worst-port choices: compare
-    # where the choice is not a near tie
-    keep = margin >= 1e-4
+        assert keep[:, s].mean() > 0.99
+        assert rel_err(out[:, s][keep[:, s]], ref[:, s][keep[:, s]]) < 1e-5, s
     for s in range(4, 8):
-        assert rel_err(out[:, s][keep], ref[:, s][keep]) < 1e-4, s
+        assert rel_err(out[:, s][keep[:, s]], ref[:, s][keep[:, s]]) < 1e-4, s
     # the reference's one-pass variance cancels where the cameras agree
     for s in range(8, 12):
-        assert rel_err(out[:, s][keep], ref[:, s][keep]) < 1e-3, s
+        assert rel_err(out[:, s][keep[:, s]], ref[:, s][keep[:, s]]) < 1e-3, s
 
 
 def test_golden_imclt(oracle, golden):
@@ -278,4 +272,5 @@ def test_golden_rgba(oracle, golden):
     assert np.array_equal(woi, d["rgba_woi"])
     h = (woi[3] + 1) * 8
     mine = np.stack([np.stack([out[s * h + r: s * h + r + 40, c: c + 40] for r, c in MG.CROPS]) for s in range(4)])
-    assert rel_err(mine, d["rgba"]) < 1e-3
+    # smooth [0, 1] scene: no unstable pixels fall in the crops
+    assert rel_err(mine, d["rgba"]) < 1e-5

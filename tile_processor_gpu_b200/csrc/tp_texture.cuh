@@ -41,14 +41,16 @@ __device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
 __device__ __forceinline__ void imclt_job(const float *__restrict__ src, const float *lpf, float *tb,
                                           float *mout, int l, unsigned gm)
 {
+    float in[4][8]; /* the job's 256 coefficients, column l of each quadrant */
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int m = 0; m < 8; m++) in[q][m] = __ldg(src + q * 64 + m * 8 + l);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         float col[8], v[8], row[8];
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
-            float x = __ldg(src + q * 64 + m * 8 + l);
-            col[m] = lpf ? x * lpf[m * 8 + l] : x;
-        }
+        for (int m = 0; m < 8; m++) col[m] = lpf ? in[q][m] * lpf[m * 8 + l] : in[q][m];
         if (q >> 1) dtt8<1>(col, v); else dtt8<0>(col, v);
 #pragma unroll
         for (int k = 0; k < 8; k++) tb[TBI(q, k, l)] = v[k];
@@ -162,7 +164,10 @@ __device__ __forceinline__ void combine_pixel(const float *sd, const float *sm, 
         }
         out[(COLORS + 5 + COLORS) * kJob + e] = sqrtf(sw);
     }
-    const float wi = (float)(1.0 / (double)wnd2);
+    /* the reference forms 1/w, the weight floor and the dust-removal scale in
+     * double; the float32 forms below give the correctly rounded reciprocal
+     * and round the floor sum once (at most one ulp from the double path) */
+    const float wi = __frcp_rn(wnd2);
     float pw[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     {
         int k = 0;
@@ -176,7 +181,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, const float *sm, 
                     const float dc = (D[i][col] - D[j][col]) * wi;
                     d = __fmaf_rn(chw[col] * dc, dc, d);
                 }
-                const float x = (float)((double)expf(-pd2r[k] * d) + 0.0001);
+                const float x = expf(-pd2r[k] * d) + 1e-4f;
                 pw[i] += x;
                 pw[j] += x;
                 k++;
@@ -215,7 +220,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, const float *sm, 
             const float dc = (D[cam][col] - avg[col]) * wi;
             d2 = __fmaf_rn(chw[col] * dc, dc, d2);
         }
-        pw[cam] = (float)((double)expf(-ksigma * d2) + 0.0001);
+        pw[cam] = expf(-ksigma * d2) + 1e-4f;
     }
     if (dust_remove) {
         int worst = 0;
@@ -228,7 +233,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, const float *sm, 
 #pragma unroll
         for (int cam = 0; cam < 4; cam++) a += pw[cam];
         a /= 3.0f;
-        const float scale = (float)(1.0 + (double)(wv * (a - wv) / (a * a * 3.0f)));
+        const float scale = 1.0f + wv * (a - wv) / (a * a * 3.0f);
         const float fw = wv / a;
 #pragma unroll
         for (int cam = 0; cam < 4; cam++) pw[cam] *= (cam == worst) ? fw : scale;
@@ -236,7 +241,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, const float *sm, 
     float ksum = 0.0f;
 #pragma unroll
     for (int cam = 0; cam < 4; cam++) ksum += pw[cam];
-    const float kinv = (float)(1.0 / (double)ksum);
+    const float kinv = __frcp_rn(ksum);
 #pragma unroll
     for (int col = 0; col < COLORS; col++) {
         float v = 0.0f;
