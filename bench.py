@@ -1,10 +1,14 @@
 """Benchmark: full-frame quad-camera CLT + correlation + texture, frames/s.
 
 One step = one 2592x1936 quad-camera Bayer frame (78,408 tiles) through the
-hot path, on inputs already resident in HBM:
+hot path, on inputs already resident in HBM, through the three drop-in entry
+points:
   1. tp_convert_correct_tiles  forward CLT + aberration kernels + shifts
   2. tp_correlate2D            6 camera pairs per tile, 15x15 outputs
   3. tp_generate_RBGA          texture list + overlapped RGBA texture
+The same frame through tp_process_frame (one kernel per tile parity with the
+tile's CLT kept in shared memory) is timed too and reported as
+`fused_frame_ms`.
 `value` is whole-job frames/s (N GPUs each process their own frames:
 frame-level replicas, weak scaling).  `e2e` is the same pipeline driven
 through the public API with host buffers: each step copies the frame's four
@@ -38,8 +42,17 @@ CORR_RADIUS = 7
 FAT_ZERO = 0.05
 TEXTURE = dict(colors=3, is_lwir=0, min_shot=10.0, scale_shot=3.0, diff_sigma=1.5, diff_threshold=10.0,
                min_agree=3.0, weight0=0.294118, weight1=0.117647, weight2=0.588235, dust_remove=1, keep_weights=0)
-WORKLOAD = ("full-frame quad 2592x1936 Bayer (78,408 tiles): convert_correct_tiles + correlate2D "
-            "(6 pairs, 15x15) + generate_RBGA (texture list + overlapped RGBA)")
+WORKLOAD = ("full-frame quad 2592x1936 Bayer (78,408 tiles): forward CLT + aberration correction, "
+            "6-pair correlation (15x15), texture list + overlapped RGBA texture")
+
+
+# dense 8x8 mat-vec flops per tile of each stage (2 flop per MAC)
+FLOPS_PER_TILE = {"convert": 75776, "correlate": 92016, "texture": 149304}
+# FP32 SIMT: 148 SMs x 128 lanes x 2 flop x 1.965 GHz
+FP32_NOMINAL_TFLOPS = 74.4
+# DRAM bytes per launch-set of each stage from an ncu capture of this workload
+# (dram__bytes_read.sum + dram__bytes_write.sum summed over the stage's kernels)
+TRAFFIC = {}
 
 
 def peaks():
@@ -171,6 +184,8 @@ class FramePipeline:
         self.corr_size = (2 * CORR_RADIUS + 1) ** 2
         self.corr_stride = self.corr_size
         self.corrs = torch.empty((self.num_corr, self.corr_stride), dtype=torch.float32, device=device)
+        # fused path: one slot per (task, pair)
+        self.corrs6 = torch.empty((self.num_tiles, 6, self.corr_stride), dtype=torch.float32, device=device)
         self.tex_indices = torch.empty(self.TX * self.TYA, dtype=torch.int32, device=device)
         self.num_tex = torch.empty(8, dtype=torch.int32, device=device)
         self.woi = torch.empty(4, dtype=torch.int32, device=device)
@@ -210,16 +225,34 @@ class FramePipeline:
                                t["scale_shot"], t["diff_sigma"], t["diff_threshold"], t["min_agree"], t["weight0"],
                                t["weight1"], t["weight2"], t["dust_remove"], 0, self.rgba_stride, self.rgba)
 
+    def frame(self):
+        t = TEXTURE
+        self.api.process_frame(self.g, self.p_extra, self.p_kernels, self.p_images, self.dstride, self.tasks,
+                               self.num_tiles, self.corrs6, self.corr_stride, self.port_offsets, self.tex_indices,
+                               self.num_tex, self.woi, self.rgba_stride, self.rgba, corr_colors=3, scale0=0.25,
+                               scale1=0.25, scale2=0.5, fat_zero=FAT_ZERO, corr_radius=CORR_RADIUS,
+                               min_shot=t["min_shot"], scale_shot=t["scale_shot"], diff_sigma=t["diff_sigma"],
+                               weight0=t["weight0"], weight1=t["weight1"], weight2=t["weight2"],
+                               dust_remove=t["dust_remove"])
+
     STAGES = ("convert", "correlate", "texture")
     LAUNCHES = {"convert": 1, "correlate": 1, "texture": 15}
+    FRAME_LAUNCHES = 11  # 6 list kernels, RGBA clear, 4 parity launches
 
     def step(self):
         self.convert()
         self.correlate()
         self.texture()
 
+    def frame_bytes(self):
+        """compulsory HBM bytes of one frame through the fused path: images,
+        touched kernel tiles and offsets, tasks, correlation out, RGBA out"""
+        T = self.num_tiles
+        return (4 * WIDTH * HEIGHT * 4 + self.kernel_tiles_touched * (1024 + 32) + T * 40 +
+                self.num_corr * self.corr_size * 4 + (self.TX + 1) * 8 * (self.TY + 1) * 8 * 4 * 4)
+
     def algorithmic_bytes(self):
-        """compulsory HBM bytes of each stage of one frame"""
+        """compulsory HBM bytes of each drop-in stage of one frame"""
         T = self.num_tiles
         clt = 4 * T * 3 * 1024
         return {
@@ -264,6 +297,20 @@ def run_b200(args, rank, world, local, pg):
     ms_max = max_over_ranks(pg, ms)
     stage_ms = {s: sum(a.elapsed_time(b) for a, b in ev[s]) / args.steps for s in pipe.STAGES}
 
+    # the same frame through tp_process_frame (fused per tile), reported beside
+    fused_steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        pipe.frame()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(fused_steps):
+        pipe.frame()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    fused_ms = f0.elapsed_time(f1) / fused_steps
+
     # ---- end to end through the public API with host buffers ----
     e2e_steps = max(2, min(args.steps, 10))
     h2d = sum(h.numel() * 4 for h in pipe.host_images)
@@ -287,21 +334,26 @@ def run_b200(args, rank, world, local, pg):
     if rank != 0:
         return None
     hbm, peak_kind = peaks()
-    dom = max(stage_ms, key=stage_ms.get)
     algo = pipe.algorithmic_bytes()
+    dom = max(stage_ms, key=stage_ms.get)
     achieved = algo[dom] / (stage_ms[dom] * 1e-3) / 1e9
     fps = world * args.steps / (ms_max * 1e-3)
+    flops = FLOPS_PER_TILE[dom] * pipe.num_tiles
     out = {
         "metric": METRIC, "value": round(fps, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plane scene, PSF kernels)",
         "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "tiles": pipe.num_tiles,
                    "corr_tiles": pipe.num_corr, "parallelism": "frame replicas x%d" % world,
+                   "path": "tp_convert_correct_tiles + tp_correlate2D + tp_generate_RBGA",
                    "l2": "per-step working set %.2f GB > 126 MB L2 (no flush)" % (sum(algo.values()) / 1e9)},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
-                     "algorithmic_bytes": int(algo[dom]), "traffic": None},
+        "fused_frame_ms": round(fused_ms, 4),
+        "roofline": {"bound": "hbm", "kernel": "k_textures (%s stage)" % dom, "achieved": round(achieved, 1),
+                     "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes": int(algo[dom]), "traffic": TRAFFIC.get(dom),
+                     "fp32_simt": {"flops": int(flops), "achieved_tflops": round(flops / (stage_ms[dom] * 1e-3) / 1e12, 2),
+                                   "nominal_peak_tflops": FP32_NOMINAL_TFLOPS}},
         "e2e": {"value": round(world / (e2e_ms * 1e-3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(args.steps * sum(pipe.LAUNCHES.values())),

@@ -238,6 +238,33 @@ int tp_generate_RBGA(const tp_geometry *g,
                      size_t texture_rbga_stride, float *texture_tiles,
                      tp_stream_t stream);
 
+/* ---- the whole hot path for one frame ------------------------------------------
+ * No single counterpart in the reference: it runs convert_correct_tiles,
+ * correlate2D and generate_RBGA (src/TileProcessor.cuh:1859-1937, :1176-1443,
+ * :1446-1615) through a device CLT buffer.  Here every tile is converted,
+ * correlated and textured by one block with its CLT in shared memory, in four
+ * launches by 2x2 tile parity.  Same inputs as tp_convert_correct_tiles, then:
+ *   corrs   : device float[num_tiles][6][corr_stride]; slot (n, pair) holds
+ *             the (2r+1)^2 correlation of task n's pair when bit 4+pair of
+ *             its task is set (other slots untouched)
+ *   texture : the texture list and window of interest of tp_generate_RBGA
+ *             (texture_indices, num_texture_tiles, woi; tasks' bits 0..3
+ *             rewritten with the neighbour mask) and its overlapped RGBA
+ *             image, 3 colours + alpha (keep_weights = 0)
+ *   clt     : optional (NULL = not written) CLT output, layout of
+ *             tp_convert_correct_tiles */
+int tp_process_frame(const tp_geometry *g,
+                     float *const *kernel_offsets, float *const *kernels, float *const *images,
+                     size_t dstride, tp_task *tasks, int num_tiles, int lpf_mask,
+                     int corr_colors, float corr_scale0, float corr_scale1, float corr_scale2,
+                     float fat_zero, int corr_radius, size_t corr_stride, float *corrs,
+                     const float *port_offsets, float min_shot, float scale_shot, float diff_sigma,
+                     float weight0, float weight1, float weight2, int dust_remove,
+                     int *texture_indices, int *num_texture_tiles, int *woi,
+                     size_t texture_rbga_stride, float *texture_rbga,
+                     float *const *clt,
+                     tp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

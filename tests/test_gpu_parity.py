@@ -208,6 +208,11 @@ def assert_close_on(b, o, keep, tol, max_frac, hard=1e-3):
         assert err.max() < hard, float(err.max())
 
 
+# A pixel of the overlapped RGBA image sums four tiles, each of which may hold
+# one of the per-tile near-tie pixels that the 1e-4 fraction above allows.
+RGBA_MAX_FRAC = 4e-4
+
+
 def _check_slices(b, o, keep, ncol, rms_tol):
     for s in range(b.shape[1]):
         if s <= ncol:
@@ -347,7 +352,7 @@ def test_rgba_vs_oracle(frames, clts, oracle, name):
     assert np.array_equal(woi, woi_o)
     h, w = _rgba_region(woi)
     keep = _rgba_stable(oracle, fr, clt, woi)
-    assert_close_on(b[:4 * h, :w], o[:4 * h, :w], keep, TOL, 1e-4)
+    assert_close_on(b[:4 * h, :w], o[:4 * h, :w], keep, TOL, RGBA_MAX_FRAC)
 
 
 @pytest.mark.parametrize("name", ["A256ref", "B512plane", "E512hdr"])
@@ -361,7 +366,7 @@ def test_rgba_vs_reference(frames, clts, oracle, name):
     assert np.array_equal(woi, woi_r)
     h, w = _rgba_region(woi)
     keep = _rgba_stable(oracle, fr, clt, woi)
-    assert_close_on(b[:4 * h, :w], r[:4 * h, :w], keep, TOL, 1e-4)
+    assert_close_on(b[:4 * h, :w], r[:4 * h, :w], keep, TOL, RGBA_MAX_FRAC)
 
 
 def test_custom_lpf_tables(frames, clts, oracle):
@@ -459,3 +464,48 @@ def test_golden_all_stages(golden):
     h = (woi[3] + 1) * 8
     mine = np.stack([np.stack([rb[s * h + r: s * h + r + 40, c: c + 40] for r, c in MG.CROPS]) for s in range(4)])
     assert rel_err(mine, d["rgba"]) < TOL
+
+
+# ---- the fused frame path ---------------------------------------------------
+
+@pytest.mark.parametrize("name", ["A256ref", "B512plane", "D256sparse", "E512hdr"])
+def test_process_frame_matches_stage_kernels(frames, name):
+    """tp_process_frame gives the drop-in pipeline's results: CLT and
+    correlations bit-identical (same device code), the overlapped RGBA within
+    1e-6 (per-pixel accumulation order differs: parity launches instead of
+    inner/border passes)."""
+    import torch
+    R = _R()
+    from tile_processor_gpu_b200 import api
+    fr = frames[name]
+    c = fr.case
+    clt_ref = R.convert(fr)
+    fr.set_clt(clt_ref)
+    corr_ref = R.correlate(fr, c.corr_idx, stride=225)
+    rgba_ref, woi_ref, stride, rows = R.rgba(fr)
+    # fused
+    n = c.num_tiles
+    tasks = api.tasks_to_device(c.tasks)
+    corrs = torch.full((n, 6, 225), -7.0, device="cuda")
+    idx = torch.zeros(c.TX * c.TYA, dtype=torch.int32, device="cuda")
+    counts = torch.zeros(8, dtype=torch.int32, device="cuda")
+    woi = torch.zeros(4, dtype=torch.int32, device="cuda")
+    rgba = torch.full((rows + 8, stride), 3.0, device="cuda")
+    clt = [torch.zeros_like(x) for x in fr.clt]
+    api.process_frame(fr.g, fr.p_extra, fr.p_kernels, fr.p_images, c.dstride, tasks, n, corrs, 225, fr.port_offsets,
+                      idx, counts, woi, stride, rgba, fat_zero=0.05, gpu_clt=clt)
+    torch.cuda.synchronize()
+    for cam in range(4):
+        assert np.array_equal(clt[cam].cpu().numpy(), clt_ref[cam])
+    # correlation slots: (task, pair) in the order of the index list
+    got = corrs.cpu().numpy()
+    tile_of_task = {}
+    for k, t in enumerate(c.tasks):
+        tile_of_task[(int(t["txy"]) & 0xFFFF) + (int(t["txy"]) >> 16) * c.TX] = k
+    for i, code in enumerate(c.corr_idx):
+        k = tile_of_task[int(code) >> 8]
+        assert np.array_equal(got[k, int(code) & 0xFF], corr_ref[i, :225]), i
+    woi_np = woi.cpu().numpy()
+    assert np.array_equal(woi_np, woi_ref)
+    h, w = _rgba_region(woi_np)
+    assert rel_err(rgba.cpu().numpy()[:4 * h, :w], rgba_ref[:4 * h, :w]) < 1e-6

@@ -165,6 +165,24 @@ def generate_RBGA(geom, gpu_tasks, num_tiles, gpu_texture_indices, num_texture_t
                  _dptr(gpu_texture_tiles), _stream(stream))
 
 
+def process_frame(geom, gpu_kernel_offsets, gpu_kernels, gpu_images, dstride, gpu_tasks, num_tiles, gpu_corrs,
+                  corr_stride, gpu_port_offsets, gpu_texture_indices, num_texture_tiles, woi, texture_rbga_stride,
+                  gpu_texture_rbga, lpf_mask=0, corr_colors=3, scale0=0.25, scale1=0.25, scale2=0.5, fat_zero=30.0,
+                  corr_radius=7, min_shot=10.0, scale_shot=3.0, diff_sigma=1.5, weight0=0.294118, weight1=0.117647,
+                  weight2=0.588235, dust_remove=1, gpu_clt=None, stream=None):
+    """One frame through the whole hot path (forward CLT, all pair
+    correlations, overlapped RGBA texture) with the CLT kept on chip.
+    gpu_corrs: [num_tiles][6][corr_stride]."""
+    clt = _parr(gpu_clt) if gpu_clt is not None else ctypes.c_void_p(0)
+    _native.call("tp_process_frame", geom.ptr, _parr(gpu_kernel_offsets), _parr(gpu_kernels), _parr(gpu_images),
+                 int(dstride), _dptr(gpu_tasks), int(num_tiles), int(lpf_mask), int(corr_colors), float(scale0),
+                 float(scale1), float(scale2), float(fat_zero), int(corr_radius), int(corr_stride), _dptr(gpu_corrs),
+                 _dptr(gpu_port_offsets), float(min_shot), float(scale_shot), float(diff_sigma), float(weight0),
+                 float(weight1), float(weight2), int(dust_remove), _dptr(gpu_texture_indices),
+                 _dptr(num_texture_tiles), _dptr(woi), int(texture_rbga_stride), _dptr(gpu_texture_rbga), clt,
+                 _stream(stream))
+
+
 def set_lpf(which, values):
     """Replace a low-pass table on the current device (0..3 lpf_data, 4 lpf_rb_corr, 5 lpf_corr)."""
     a = np.ascontiguousarray(values, dtype=np.float32).reshape(64)

@@ -17,6 +17,7 @@
 #include "tp_texture.cuh"
 #include "tp_imclt.cuh"
 #include "tp_list.cuh"
+#include "tp_frame.cuh"
 
 #define TP_VERSION "tile_processor_gpu_b200 0.1 (sm_100a)"
 
@@ -343,6 +344,66 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
                                             texture_tiles, 0, nullptr);
     }
     return cuda_status(cudaGetLastError(), "generate_RBGA launch");
+}
+
+int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *const *kernels, float *const *images,
+                     size_t dstride, tp_task *tasks, int num_tiles, int lpf_mask, int corr_colors, float corr_scale0,
+                     float corr_scale1, float corr_scale2, float fat_zero, int corr_radius, size_t corr_stride,
+                     float *corrs, const float *port_offsets, float min_shot, float scale_shot, float diff_sigma,
+                     float weight0, float weight1, float weight2, int dust_remove, int *texture_indices,
+                     int *num_texture_tiles, int *woi, size_t texture_rbga_stride, float *texture_rbga,
+                     float *const *clt, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (!kernel_offsets || !kernels || !images) return fail(TP_ERR_ARG, "NULL pointer array");
+    if (num_tiles < 0) return fail(TP_ERR_ARG, "num_tiles %d < 0", num_tiles);
+    if (dstride < (size_t)g->img_width) return fail(TP_ERR_ARG, "dstride %zu < width %d", dstride, g->img_width);
+    if (corr_colors != 1 && corr_colors != 3) return fail(TP_ERR_ARG, "corr_colors %d (1 or 3)", corr_colors);
+    if (corr_radius < 0 || corr_radius > TP_MAX_CORR_RADIUS)
+        return fail(TP_ERR_ARG, "corr_radius %d outside 0..%d", corr_radius, TP_MAX_CORR_RADIUS);
+    const size_t sz = (size_t)(2 * corr_radius + 1) * (2 * corr_radius + 1);
+    if (corr_stride < sz) return fail(TP_ERR_ARG, "corr_stride %zu < (2r+1)^2 = %zu", corr_stride, sz);
+    tp::TextureParams tex;
+    if ((rc = texture_params(3, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2, dust_remove, 0, &tex)))
+        return rc;
+    if (texture_rbga_stride < (size_t)(gd.TX + 1) * 8)
+        return fail(TP_ERR_ARG, "texture_rbga_stride %zu < (tilesx + 1) * 8", texture_rbga_stride);
+    if (!corrs || !port_offsets || !texture_rbga) return fail(TP_ERR_ARG, "NULL corrs / port_offsets / texture_rbga");
+    if (num_tiles == 0) return TP_OK;
+    if ((rc = tp_prepare_texture_list(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, gd.TX, gd.TY,
+                                      stream)))
+        return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    {
+        const int max_rows = (gd.TY + 1) * 8 * 4;
+        dim3 grid((unsigned)(((gd.TX + 2) * 8 + 255) / 256), (unsigned)(max_rows < 65535 ? max_rows : 65535), 1);
+        tp::k_clear_rbga<<<grid, 256, 0, s>>>(woi, 3, 0, 0, texture_rbga_stride, texture_rbga);
+    }
+    tp::FrameParams fp;
+    fp.lpf_mask = lpf_mask;
+    fp.corr_colors = corr_colors;
+    fp.s0 = corr_scale0;
+    fp.s1 = corr_scale1;
+    fp.s2 = corr_scale2;
+    fp.fat_zero = fat_zero;
+    fp.corr_radius = corr_radius;
+    fp.corr_stride = corr_stride;
+    fp.tex = tex;
+    /* odd grid: a grid-stride walk over a raster task list then visits both
+     * column parities in every block */
+    if ((rc = cuda_status(cudaFuncSetAttribute(tp::k_frame, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)tp::kFrameSmemBytes),
+                          "cudaFuncSetAttribute(k_frame)")))
+        return rc;
+    unsigned grid = grid_for(num_tiles, 4, sms, 3) | 1u;
+    for (int parity = 0; parity < 4; parity++)
+        tp::k_frame<<<grid, 128, tp::kFrameSmemBytes, s>>>(gd, dstride, kernel_offsets, kernels, images, tasks, num_tiles, parity, fp,
+                                         corrs, port_offsets, woi, texture_rbga_stride, texture_rbga, clt);
+    return cuda_status(cudaGetLastError(), "process_frame launch");
 }
 
 } /* extern "C" */

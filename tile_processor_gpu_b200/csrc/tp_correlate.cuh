@@ -22,12 +22,102 @@ namespace tp {
  * quadrants), then the (2r+1)^2 output staging; 536 % 32 == 24 */
 constexpr int kCorrBuf = 4 * 72 + 8 + 240;
 
+/* One (tile, pair) correlation on an 8-lane group.  a, b: the two cameras'
+ * CLT of the tile, colour c at a + c * cstride (4 x 64 floats, row stride 8);
+ * global or shared.  tb: kCorrBuf floats of this group.  dst: (2r+1)^2
+ * floats. */
+__device__ __forceinline__ void corr_job(const float *a, const float *b, int cstride, int colors, float scale0,
+                                         float scale1, float scale2, float fat_zero, int r, float *tb,
+                                         float *__restrict__ dst, int l, unsigned gm)
+{
+    const int sz = 2 * r + 1;
+    float *stage = tb + 296;
+    float acc[4][8];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int m = 0; m < 8; m++) acc[q][m] = 0.0f;
+    for (int color = 0; color < colors; color++) {
+        const float s = color == 0 ? scale0 : color == 1 ? scale1 : scale2;
+        const float *ta = a + color * cstride + l, *tbb = b + color * cstride + l;
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const int o = m * 8;
+            const float a0 = ta[o], a1 = ta[o + 64], a2 = ta[o + 128], a3 = ta[o + 192];
+            const float b0 = tbb[o], b1 = tbb[o + 64], b2 = tbb[o + 128], b3 = tbb[o + 192];
+            /* CLT-domain correlation of the two tiles */
+            const float r0 = __fmaf_rn(a3, b3, __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, a0 * b0)));
+            const float r1 = __fmaf_rn(a2, b3, __fmaf_rn(-a3, b2, __fmaf_rn(a0, b1, -a1 * b0)));
+            const float r2 = __fmaf_rn(a1, b3, __fmaf_rn(a0, b2, __fmaf_rn(-a3, b1, -a2 * b0)));
+            const float r3 = __fmaf_rn(a0, b3, __fmaf_rn(-a1, b2, __fmaf_rn(-a2, b1, a3 * b0)));
+            acc[0][m] = __fmaf_rn(s, r0, acc[0][m]);
+            acc[1][m] = __fmaf_rn(s, r1, acc[1][m]);
+            acc[2][m] = __fmaf_rn(s, r2, acc[2][m]);
+            acc[3][m] = __fmaf_rn(s, r3, acc[3][m]);
+        }
+        if (color == 1) { /* LPF after red and blue */
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const float f = c_lpf[4][m * 8 + l];
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[q][m] *= f;
+            }
+        }
+    }
+    /* amplitude normalisation with fat zero, then the final LPF */
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        float s2 = fat_zero * fat_zero;
+#pragma unroll
+        for (int q = 0; q < 4; q++) s2 = __fmaf_rn(acc[q][m], acc[q][m], s2);
+        const float sc = rsqrtf(s2);
+        const float f = c_lpf[5][m * 8 + l];
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[q][m] = (acc[q][m] * sc) * f;
+    }
+    /* pixel domain: vertical DCT-II (q0,q1) / DST-II (q2,q3) on the held
+     * column, transpose, horizontal DCT-II (q0,q2) / DST-II (q1,q3); the
+     * result row l of quadrant q replaces its transpose buffer */
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        float v[8], row[8];
+        if (q >> 1) dtt8<3>(acc[q], v); else dtt8<2>(acc[q], v);
+#pragma unroll
+        for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
+        __syncwarp(gm);
+#pragma unroll
+        for (int k = 0; k < 8; k++) row[k] = tb[TBI(q, k, l)];
+        __syncwarp(gm);
+        if (q & 1) dtt8<3>(row, v); else dtt8<2>(row, v);
+#pragma unroll
+        for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
+    }
+    __syncwarp(gm);
+    /* unfold (lane i = rows +-i): R[+-i][+-j] from q0[i][j], q1[i][j-1],
+     * q2[i-1][j], q3[i-1][j-1], scaled by 1/4 */
+    if (l <= r) {
+        for (int j = 0; j <= r; j++) {
+            const float q0 = tb[TBI(0, l, j)];
+            const float q1 = j > 0 ? tb[TBI(1, l, j - 1)] : 0.0f;
+            const float q2 = l > 0 ? tb[TBI(2, l - 1, j)] : 0.0f;
+            const float q3 = (l > 0 && j > 0) ? tb[TBI(3, l - 1, j - 1)] : 0.0f;
+            stage[(r + l) * sz + (r + j)] = 0.25f * ((q0 + q1) + (q2 + q3));
+            stage[(r + l) * sz + (r - j)] = 0.25f * ((q0 - q1) + (q2 - q3));
+            stage[(r - l) * sz + (r + j)] = 0.25f * ((q0 + q1) - (q2 + q3));
+            stage[(r - l) * sz + (r - j)] = 0.25f * ((q0 - q1) - (q2 - q3));
+        }
+    }
+    __syncwarp(gm);
+    for (int k = l; k < sz * sz; k += 8) dst[k] = stage[k];
+    __syncwarp(gm);
+}
+
 __global__ void __launch_bounds__(128, 3) k_correlate2D(Geom g, float *const *clt, int colors,
-                                                     float scale0, float scale1, float scale2,
-                                                     float fat_zero, long long num_corr_tiles,
-                                                     const int *__restrict__ corr_indices,
-                                                     size_t corr_stride, int corr_radius,
-                                                     float *__restrict__ corrs)
+                                                        float scale0, float scale1, float scale2,
+                                                        float fat_zero, long long num_corr_tiles,
+                                                        const int *__restrict__ corr_indices,
+                                                        size_t corr_stride, int corr_radius,
+                                                        float *__restrict__ corrs)
 {
     __shared__ float tbuf[128 / 8][kCorrBuf];
     const int l = threadIdx.x & 7;
@@ -35,93 +125,14 @@ __global__ void __launch_bounds__(128, 3) k_correlate2D(Geom g, float *const *cl
     const unsigned gm = group_mask();
     const long long groups_total = (long long)gridDim.x * (blockDim.x >> 3);
     const int ntiles = g.TX * g.TY;
-    const int r = corr_radius, sz = 2 * r + 1;
-    float *tb = tbuf[grp];
-    float *stage = tb + 296;
     for (long long n = (long long)blockIdx.x * (blockDim.x >> 3) + grp; n < num_corr_tiles; n += groups_total) {
         const int code = corr_indices[n];
         const int tile = code >> 8, pair = code & 0xff;
         if (pair >= 6 || tile < 0 || tile >= ntiles) continue;
-        const float *ta = clt[c_pairs[pair][0]] + (size_t)tile * 768 + l;
-        const float *tb2 = clt[c_pairs[pair][1]] + (size_t)tile * 768 + l;
-        float acc[4][8];
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-#pragma unroll
-            for (int m = 0; m < 8; m++) acc[q][m] = 0.0f;
-        for (int color = 0; color < colors; color++) {
-            const float s = color == 0 ? scale0 : color == 1 ? scale1 : scale2;
-#pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const int o = color * 256 + m * 8;
-                const float a0 = __ldg(ta + o), a1 = __ldg(ta + o + 64), a2 = __ldg(ta + o + 128), a3 = __ldg(ta + o + 192);
-                const float b0 = __ldg(tb2 + o), b1 = __ldg(tb2 + o + 64), b2 = __ldg(tb2 + o + 128), b3 = __ldg(tb2 + o + 192);
-                /* CLT-domain correlation of the two tiles */
-                const float r0 = __fmaf_rn(a3, b3, __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, a0 * b0)));
-                const float r1 = __fmaf_rn(a2, b3, __fmaf_rn(-a3, b2, __fmaf_rn(a0, b1, -a1 * b0)));
-                const float r2 = __fmaf_rn(a1, b3, __fmaf_rn(a0, b2, __fmaf_rn(-a3, b1, -a2 * b0)));
-                const float r3 = __fmaf_rn(a0, b3, __fmaf_rn(-a1, b2, __fmaf_rn(-a2, b1, a3 * b0)));
-                acc[0][m] = __fmaf_rn(s, r0, acc[0][m]);
-                acc[1][m] = __fmaf_rn(s, r1, acc[1][m]);
-                acc[2][m] = __fmaf_rn(s, r2, acc[2][m]);
-                acc[3][m] = __fmaf_rn(s, r3, acc[3][m]);
-            }
-            if (color == 1) { /* LPF after red and blue */
-#pragma unroll
-                for (int m = 0; m < 8; m++) {
-                    const float f = c_lpf[4][m * 8 + l];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) acc[q][m] *= f;
-                }
-            }
-        }
-        /* amplitude normalisation with fat zero, then the final LPF */
-#pragma unroll
-        for (int m = 0; m < 8; m++) {
-            float s2 = fat_zero * fat_zero;
-#pragma unroll
-            for (int q = 0; q < 4; q++) s2 = __fmaf_rn(acc[q][m], acc[q][m], s2);
-            const float sc = rsqrtf(s2);
-            const float f = c_lpf[5][m * 8 + l];
-#pragma unroll
-            for (int q = 0; q < 4; q++) acc[q][m] = (acc[q][m] * sc) * f;
-        }
-        /* pixel domain: vertical DCT-II (q0,q1) / DST-II (q2,q3) on the held
-         * column, transpose, horizontal DCT-II (q0,q2) / DST-II (q1,q3); the
-         * result row l of quadrant q replaces its transpose buffer */
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            float v[8], row[8];
-            if (q >> 1) dtt8<3>(acc[q], v); else dtt8<2>(acc[q], v);
-#pragma unroll
-            for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
-            __syncwarp(gm);
-#pragma unroll
-            for (int k = 0; k < 8; k++) row[k] = tb[TBI(q, k, l)];
-            __syncwarp(gm);
-            if (q & 1) dtt8<3>(row, v); else dtt8<2>(row, v);
-#pragma unroll
-            for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
-        }
-        __syncwarp(gm);
-        /* unfold (lane i = rows +-i): R[+-i][+-j] from q0[i][j], q1[i][j-1],
-         * q2[i-1][j], q3[i-1][j-1], scaled by 1/4 */
-        if (l <= r) {
-            for (int j = 0; j <= r; j++) {
-                const float q0 = tb[TBI(0, l, j)];
-                const float q1 = j > 0 ? tb[TBI(1, l, j - 1)] : 0.0f;
-                const float q2 = l > 0 ? tb[TBI(2, l - 1, j)] : 0.0f;
-                const float q3 = (l > 0 && j > 0) ? tb[TBI(3, l - 1, j - 1)] : 0.0f;
-                stage[(r + l) * sz + (r + j)] = 0.25f * ((q0 + q1) + (q2 + q3));
-                stage[(r + l) * sz + (r - j)] = 0.25f * ((q0 - q1) + (q2 - q3));
-                stage[(r - l) * sz + (r + j)] = 0.25f * ((q0 + q1) - (q2 + q3));
-                stage[(r - l) * sz + (r - j)] = 0.25f * ((q0 - q1) - (q2 - q3));
-            }
-        }
-        __syncwarp(gm);
-        float *dst = corrs + (size_t)n * corr_stride;
-        for (int k = l; k < sz * sz; k += 8) dst[k] = stage[k];
-        __syncwarp(gm);
+        const float *ta = clt[c_pairs[pair][0]] + (size_t)tile * 768;
+        const float *tb2 = clt[c_pairs[pair][1]] + (size_t)tile * 768;
+        corr_job(ta, tb2, 256, colors, scale0, scale1, scale2, fat_zero, corr_radius, tbuf[grp],
+                 corrs + (size_t)n * corr_stride, l, gm);
     }
 }
 

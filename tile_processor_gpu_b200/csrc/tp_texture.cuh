@@ -8,10 +8,10 @@
  * job one 8-lane group, working only with __syncwarp on its own buffers:
  *   1. low-pass filter and invert the CLT tile (vertical DCT-IV/DST-IV on the
  *      held column, transpose, horizontal pass on the held row) and unfold it
- *      into the windowed 16x16 tile M;
- *   2. un-window M, debayer the interior with the 3x3 stencil, apply the
- *      shot-noise square root and re-window into D (lane l owns columns l and
- *      l + 8).
+ *      into the windowed 16x16 tile M and the un-windowed tile T;
+ *   2. debayer T with the 3x3 stencil (a register window walked down each
+ *      column), apply the shot-noise square root and re-window into D (lane l
+ *      owns columns l and l + 8).
  * After one block barrier every thread fuses the four cameras at two pixels
  * (stage 3), and the slices are written as non-overlapping 16x16 tiles and/or
  * faded by the neighbour mask and added into the overlapped RGBA image
@@ -35,17 +35,22 @@ constexpr int kJob = 280;        /* floats per 16x17 job tile, padded */
 
 __device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
 
-/* windowed inverse CLT of one job into a [16][17] tile (w * d, no accumulate).
- * Quadrant signs of the unfold (idct_signs, src/TileProcessor.cuh:399-420)
- * factor into a vertical and a horizontal sign vector. */
-__device__ __forceinline__ void imclt_job(const float *__restrict__ src, const float *lpf, float *tb,
-                                          float *mout, int l, unsigned gm)
+/* Windowed inverse CLT of one job (imclt8threads, :3847-4017) into the
+ * [16][17] tile M = w * d (w the product of the two half-sine windows, no
+ * accumulation), and, for the debayer, the same tile with the squared window
+ * removed, T = M / (sin^2 r sin^2 c) = d / (4 sin r sin c), formed directly
+ * from the signed sum d.  The quadrant signs of the unfold (idct_signs,
+ * :399-420) factor into a vertical and a horizontal sign vector.  src: the
+ * job's 4x64 coefficients (row stride 8), global or shared.  tout may be
+ * NULL (no debayer). */
+__device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *mout,
+                                                 float *tout, int l, unsigned gm)
 {
     float in[4][8]; /* the job's 256 coefficients, column l of each quadrant */
 #pragma unroll
     for (int q = 0; q < 4; q++)
 #pragma unroll
-        for (int m = 0; m < 8; m++) in[q][m] = __ldg(src + q * 64 + m * 8 + l);
+        for (int m = 0; m < 8; m++) in[q][m] = src[q * 64 + m * 8 + l];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         float col[8], v[8], row[8];
@@ -73,59 +78,70 @@ __device__ __forceinline__ void imclt_job(const float *__restrict__ src, const f
         const int cq = c >> 2;
         const float shc = (cq == 0) ? 1.0f : -1.0f; /* cosine horizontal */
         const float shs = (cq == 3) ? -1.0f : 1.0f; /* sine horizontal   */
-        const float wc = 0.5f * c_hwin[c];
+        const float hc = c_hwin[c];
+        const float wc = 0.5f * hc;
+        const float tc = 0.25f / hc;
+        const float *col = tb + v;
 #pragma unroll
         for (int r = 0; r < 16; r++) {
             const int u = (r < 4) ? r + 4 : (r < 12) ? 11 - r : r - 12;
             const int rq = r >> 2;
-            const float svc = (rq == 0) ? 1.0f : -1.0f;
-            const float svs = (rq == 3) ? -1.0f : 1.0f;
-            const float d01 = (svc * shc) * tb[TBI(0, u, v)] + (svc * shs) * tb[TBI(1, u, v)];
-            const float d23 = (svs * shc) * tb[TBI(2, u, v)] + (svs * shs) * tb[TBI(3, u, v)];
-            const float w = (0.5f * c_hwin[r]) * wc;
-            mout[JT(r, c)] = w * (d01 + d23);
+            const float a0 = col[TBI(0, u, 0)], a1 = col[TBI(1, u, 0)];
+            const float a2 = col[TBI(2, u, 0)], a3 = col[TBI(3, u, 0)];
+            /* (+/-shc) a0 + (+/-shs) a1 with the vertical sign known here */
+            const float d01 = (rq == 0) ? __fmaf_rn(shs, a1, shc * a0) : -__fmaf_rn(shs, a1, shc * a0);
+            const float d23 = (rq == 3) ? -__fmaf_rn(shs, a3, shc * a2) : __fmaf_rn(shs, a3, shc * a2);
+            const float d = d01 + d23;
+            mout[JT(r, c)] = ((0.5f * c_hwin[r]) * wc) * d;
+            if (tout) tout[JT(r, c)] = d * (tc / c_hwin[r]);
         }
     }
 }
 
-/* un-window, 3x3 debayer (interior 14x14; border copied), shot-noise square
- * root, re-window: M -> D through the scratch tile T.  Lane l: columns l and
- * l + 8.  hsq = sin^2 of the window, hsqi = its reciprocal. */
-__device__ __forceinline__ void debayer_job(const float *m, float *t, float *d, int rb_mode, float min_shot,
-                                            float scale_shot, const float *hsq, const float *hsqi, int l,
-                                            unsigned gm)
+/* 3x3 debayer of the un-windowed tile T (interior 14x14; border copied),
+ * shot-noise square root, squared window re-applied: T -> D
+ * (debayer_shot / debayer, :4019-4199).  Lane l: columns l and l + 8, each
+ * walked down with a 3x3 register window. */
+__device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mode, float min_shot,
+                                            float scale_shot, int l, unsigned gm)
 {
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-        const int c = l + 8 * h;
-        const float wx = hsqi[sym8(c)];
-#pragma unroll
-        for (int r = 0; r < 16; r++) t[JT(r, c)] = (m[JT(r, c)] * wx) * hsqi[sym8(r)];
-    }
     __syncwarp(gm);
     const float kshot = rsqrtf(min_shot);
 #pragma unroll 1
     for (int h = 0; h < 2; h++) {
         const int c = l + 8 * h;
-        const float wx = hsq[sym8(c)];
         const bool cborder = (c == 0) || (c == 15);
+        const int cm = cborder ? c : c - 1, cp = cborder ? c : c + 1;
+        const float hcc = c_hwin[c];
+        const float wx = hcc * hcc;
+        float a0 = t[JT(0, cm)], a1 = t[JT(0, c)], a2 = t[JT(0, cp)];
+        float b0 = t[JT(1, cm)], b1 = t[JT(1, c)], b2 = t[JT(1, cp)];
 #pragma unroll
         for (int r = 0; r < 16; r++) {
             float v;
-            if (cborder || r == 0 || r == 15) {
-                v = t[JT(r, c)];
+            if (r == 0) {
+                v = a1;
+            } else if (r == 15) {
+                v = b1;
             } else {
-                const float orth = ((t[JT(r - 1, c)] + t[JT(r + 1, c)]) + t[JT(r, c - 1)]) + t[JT(r, c + 1)];
-                if (rb_mode) {
-                    const float diag = ((t[JT(r - 1, c - 1)] + t[JT(r - 1, c + 1)]) + t[JT(r + 1, c - 1)]) +
-                                       t[JT(r + 1, c + 1)];
-                    v = __fmaf_rn(0.0625f, diag, __fmaf_rn(0.125f, orth, 0.25f * t[JT(r, c)]));
+                const float e0 = t[JT(r + 1, cm)], e1 = t[JT(r + 1, c)], e2 = t[JT(r + 1, cp)];
+                if (cborder) {
+                    v = b1;
                 } else {
-                    v = __fmaf_rn(0.125f, orth, 0.5f * t[JT(r, c)]);
+                    const float orth = ((a1 + e1) + b0) + b2;
+                    if (rb_mode) {
+                        const float diag = ((a0 + a2) + e0) + e2;
+                        v = __fmaf_rn(0.0625f, diag, __fmaf_rn(0.125f, orth, 0.25f * b1));
+                    } else {
+                        v = __fmaf_rn(0.125f, orth, 0.5f * b1);
+                    }
                 }
+                a0 = b0; a1 = b1; a2 = b2;
+                b0 = e0; b1 = e1; b2 = e2;
             }
             if (scale_shot > 0.0f) v = scale_shot * ((v > min_shot) ? sqrtf(v) : (kshot * v));
-            d[JT(r, c)] = v * (wx * hsq[sym8(r)]);
+            const float hr = c_hwin[r];
+            d[JT(r, c)] = v * (wx * (hr * hr));
         }
     }
     __syncwarp(gm);
@@ -135,8 +151,8 @@ __device__ __forceinline__ void debayer_job(const float *m, float *t, float *d, 
  * D: debayered, M: plain tiles, both [job = cam * colors + color].
  * Writes colors, alpha, 4 port weights and (keep_weights) colors+1 rms. */
 template <int COLORS>
-__device__ __forceinline__ void combine_pixel(const float *sd, const float *sm, float *out, int r, int c,
-                                              const float *pd2r, float ksigma, const float *chw, float wnd2,
+__device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, const float *sm, float *out, int r,
+                                              int c, const float *pd2r, float ksigma, const float *chw, float wnd2,
                                               int dust_remove, int keep_weights)
 {
     const int e = JT(r, c);
@@ -144,7 +160,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, const float *sm, 
 #pragma unroll
     for (int cam = 0; cam < 4; cam++)
 #pragma unroll
-        for (int col = 0; col < COLORS; col++) D[cam][col] = sd[(cam * COLORS + col) * kJob + e];
+        for (int col = 0; col < COLORS; col++) D[cam][col] = sd[(cam * COLORS + col) * sd_stride + e];
     if (keep_weights) {
         float sw = 0.0f;
 #pragma unroll
@@ -261,10 +277,9 @@ __global__ void __launch_bounds__(128, 3) k_textures(
     size_t texture_rbg_stride, float *__restrict__ texture_rbg, size_t texture_stride,
     float *__restrict__ texture_tiles)
 {
-    __shared__ float s_m[12 * kJob];   /* IMCLT tiles (not debayered)              */
-    __shared__ float s_d[12 * kJob];   /* debayered tiles                          */
-    __shared__ float s_x[12 * kTB4];   /* transposes, then un-windowed tiles, then
-                                        * the output slices (12 x kJob floats)     */
+    __shared__ float s_m[12 * kJob];   /* IMCLT tiles M (not debayered)                    */
+    __shared__ float s_d[12 * kJob];   /* un-windowed tiles T, then the output slices      */
+    __shared__ float s_x[12 * kTB4];   /* transposes, then the debayered tiles D           */
     __shared__ float s_hsq[16], s_hsqi[16];
 
     const int tid = threadIdx.x;
@@ -314,30 +329,24 @@ __global__ void __launch_bounds__(128, 3) k_textures(
         if (grp < njobs) {
             const int cam = grp / colors, color = grp - cam * colors;
             const float *src = clt[cam] + ((size_t)tile * 3 + color) * 256;
-            float *mj = s_m + grp * kJob, *dj = s_d + grp * kJob, *xj = s_x + grp * kTB4;
-            imclt_job(src, c_lpf[colors > 1 ? color : 3], xj, mj, l, gm);
-            __syncwarp(gm);
-            if (colors > 1) {
-                debayer_job(mj, xj, dj, color < 2, p.min_shot, p.scale_shot, s_hsq, s_hsqi, l, gm);
-            } else {
-#pragma unroll
-                for (int r = 0; r < 16; r++) {
-                    dj[JT(r, l)] = mj[JT(r, l)];
-                    dj[JT(r, l + 8)] = mj[JT(r, l + 8)];
-                }
-            }
+            float *mj = s_m + grp * kJob, *tj = s_d + grp * kJob, *xj = s_x + grp * kTB4;
+            /* M -> s_m; the un-windowed T -> s_d; the debayered D -> s_x
+             * (the transpose buffer, free once the unfold has read it) */
+            imclt_unfold_job(src, c_lpf[colors > 1 ? color : 3], xj, mj, colors > 1 ? tj : nullptr, l, gm);
+            if (colors > 1) debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
         }
         __syncthreads();
 
-        /* ---- stage 3: fuse the four cameras, one thread per pixel ---- */
+        /* ---- stage 3: fuse the four cameras, one thread per pixel; the
+         * slices go to s_d ---- */
 #pragma unroll 1
         for (int px = tid; px < 256; px += 128) {
             const int r = px >> 4, c = px & 15;
             const float wnd2 = s_hsq[sym8(r)] * s_hsq[sym8(c)];
             if (colors == 3)
-                combine_pixel<3>(s_d, s_m, s_x, r, c, pd2r, ksigma, chw, wnd2, p.dust_remove, p.keep_weights);
+                combine_pixel<3>(s_x, kTB4, s_m, s_d, r, c, pd2r, ksigma, chw, wnd2, p.dust_remove, p.keep_weights);
             else
-                combine_pixel<1>(s_d, s_m, s_x, r, c, pd2r, ksigma, chw, wnd2, p.dust_remove, p.keep_weights);
+                combine_pixel<1>(s_m, kJob, s_m, s_d, r, c, pd2r, ksigma, chw, wnd2, p.dust_remove, p.keep_weights);
         }
         __syncthreads();
 
@@ -347,7 +356,7 @@ __global__ void __launch_bounds__(128, 3) k_textures(
             float *dst = texture_tiles + (size_t)n * texture_stride;
             for (int e = tid; e < ns * 256; e += 128) {
                 const int s = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                dst[e] = s_x[s * kJob + JT(r, c)];
+                dst[e] = s_d[s * kJob + JT(r, c)];
             }
         }
         const int nbr = code & TP_TASK_TEXTURE_BITS;
@@ -356,7 +365,7 @@ __global__ void __launch_bounds__(128, 3) k_textures(
             const long long x0 = (long long)(tx - wx0) * 8, y0 = (long long)(ty - wy0) * 8;
             for (int e = tid; e < (colors + 1) * 256; e += 128) {
                 const int s = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                float v = s_x[s * kJob + JT(r, c)];
+                float v = s_d[s * kJob + JT(r, c)];
                 if (nbr != TP_TASK_TEXTURE_BITS) v *= c_alpha_fade[nbr][r * 16 + c];
                 const long long gy = y0 + r, gx = x0 + c;
                 if (gy < 0 || gx < 0) continue;
