@@ -90,6 +90,14 @@ unsigned grid_for(long long items, int items_per_block, int sms, int per_sm)
     return (unsigned)need;
 }
 
+/* k_textures takes more than the 48 KB of shared memory granted by default */
+int texture_smem_setup()
+{
+    return cuda_status(cudaFuncSetAttribute(tp::k_textures, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)tp::kTexSmemBytes),
+                       "cudaFuncSetAttribute(k_textures)");
+}
+
 /* host copy of the low-pass tables (last values set by tp_set_lpf) */
 float g_lpf_host[6][64] = TP_LPF_DEFAULT_INIT;
 const float g_lpf_default[6][64] = TP_LPF_DEFAULT_INIT;
@@ -108,7 +116,7 @@ int tp_tiles_ya(const tp_geometry *g) { return g ? ((g->img_height / 8 + 3) & ~3
 int tp_set_lpf(int which, const float *values)
 {
     if (which < 0 || which > 5 || !values) return fail(TP_ERR_ARG, "tp_set_lpf(%d, %p)", which, values);
-    int rc = cuda_status(cudaMemcpyToSymbol(tp::c_lpf, values, 64 * sizeof(float), which * 64 * sizeof(float)),
+    int rc = cuda_status(cudaMemcpyToSymbol(tp::d_lpf, values, 64 * sizeof(float), which * 64 * sizeof(float)),
                          "cudaMemcpyToSymbol(lpf)");
     if (rc) return rc;
     memcpy(g_lpf_host[which], values, 64 * sizeof(float));
@@ -220,8 +228,9 @@ int tp_textures_accumulate(const tp_geometry *g, const int *woi, float *const *c
         return fail(TP_ERR_ARG, "texture_stride %zu < %d slices x 256", texture_stride, ns);
     int sms;
     if ((rc = sm_count(&sms))) return rc;
+    if ((rc = texture_smem_setup())) return rc;
     unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, 3);
-    tp::k_textures<<<grid, 128, 0, (cudaStream_t)stream>>>(
+    tp::k_textures<<<grid, 128, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
         gd, woi, clt, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
         want_tiles ? texture_tiles : nullptr);
@@ -335,11 +344,12 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
     }
     const int quarter = gd.TX * (gd.TYA >> 2);
     const unsigned grid = grid_for(quarter, 1, sms, 3);
+    if ((rc = texture_smem_setup())) return rc;
     for (int pass = 0; pass < 8; pass++) {
         const int border = pass >> 2;
         const int slot = ((pass & 3) << 1) + border;
         const int *base = texture_indices + (pass & 3) * quarter;
-        tp::k_textures<<<grid, 128, 0, s>>>(gd, woi, clt, 0, base, num_texture_tiles, slot, quarter,
+        tp::k_textures<<<grid, 128, tp::kTexSmemBytes, s>>>(gd, woi, clt, 0, base, num_texture_tiles, slot, quarter,
                                             border ? quarter : 0, port_offsets, p, texture_rbga_stride,
                                             texture_tiles, 0, nullptr);
     }

@@ -28,9 +28,15 @@ __device__ __constant__ float c_dst2[8][8] = TP_DST2_INIT;
 __device__ __constant__ float c_hwin[16] = TP_HWIN_INIT;
 __device__ __constant__ float c_hwinc[16] = TP_HWINC_INIT;
 __device__ __constant__ int c_rind[16] = TP_RIND_INIT;
-/* runtime-settable low-pass filters: lpf_data[0..3], lpf_rb_corr, lpf_corr */
-__device__ __constant__ float c_lpf[6][64] = TP_LPF_DEFAULT_INIT;
-__device__ __constant__ float c_alpha_fade[16][256] = TP_ALPHA_FADE_INIT;
+/* Tables that lanes index by their own row / column live in global memory
+ * and are read through the read-only data cache: the lanes of a warp then
+ * fetch distinct words in one pass, where the constant cache would serialise
+ * them.  Runtime-settable low-pass filters: lpf_data[0..3], lpf_rb_corr,
+ * lpf_corr. */
+__device__ float d_lpf[6][64] = TP_LPF_DEFAULT_INIT;
+__device__ float d_alpha_fade[16][256] = TP_ALPHA_FADE_INIT;
+__device__ float d_hwin[16] = TP_HWIN_INIT;
+__device__ float d_hwinc[16] = TP_HWINC_INIT;
 /* camera pairs (src/TileProcessor.cuh:484-490) */
 __device__ __constant__ int c_pairs[6][2] = {{0, 1}, {2, 3}, {0, 2}, {1, 3}, {0, 3}, {2, 1}};
 
@@ -50,6 +56,27 @@ constexpr int kTB4 = 4 * 72 + 8;
 #define TBI(q, r, c) ((q) * 72 + (r) * 9 + (c))
 
 __device__ __forceinline__ unsigned group_mask() { return 0xffu << (threadIdx.x & 24); }
+
+/* One (camera, colour) CLT tile staged in shared memory: 256 coefficients
+ * padded to 264 floats (264 % 32 == 8, 16-byte multiple), so the four groups
+ * of a warp reading column l of their own job hit distinct banks. */
+constexpr int kCltJob = 264;
+
+/* Asynchronous global -> shared copies (LDGSTS).  Completion is awaited with
+ * cp_async_wait_all() by the issuing thread; other threads see the data after
+ * a following block barrier. */
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 /* y[k] = sum_n M[k][n] x[n] with M a constant table */
 template <int KIND>
@@ -104,10 +131,16 @@ __device__ __forceinline__ int fold_sample(int u, int p)
 __device__ __forceinline__ float fold_sign_c(int n) { return n < 4 ? 1.0f : -1.0f; }
 __device__ __forceinline__ float fold_sign_s(int n) { return n < 12 ? 1.0f : -1.0f; }
 
-/* window value w(n + s) = sin(pi (2 (n + s) + 1) / 32) from (cos, sin)(pi s / 16) */
+/* window value w(n + s) = sin(pi (2 (n + s) + 1) / 32) from (cos, sin)(pi s / 16);
+ * n uniform across the warp */
 __device__ __forceinline__ float shifted_window(int n, float cs, float sn)
 {
     return __fmaf_rn(c_hwin[n], cs, c_hwinc[n] * sn);
+}
+/* the same with a lane-dependent n */
+__device__ __forceinline__ float shifted_window_lane(int n, float cs, float sn)
+{
+    return __fmaf_rn(__ldg(&d_hwin[n]), cs, __ldg(&d_hwinc[n]) * sn);
 }
 
 } /* namespace tp */

@@ -93,7 +93,7 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
         const int colp = (itlx & 1) ^ (1 ^ c0 ^ c1 ^ gp);
         const int rowp = (itly & 1) ^ (c0 ^ gp);
         const int lr = fold_sample(l, rowp);
-        const float wv = fold_sign_c(lr) * shifted_window(lr, vc, vs);
+        const float wv = fold_sign_c(lr) * shifted_window_lane(lr, vc, vs);
         long long rowbase;
         int eff_col = 0;
         if (fast) {
@@ -195,7 +195,7 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
     if ((lpf_mask >> color) & 1) { /* optional LPF (:3572-3593) */
 #pragma unroll
         for (int m = 0; m < 8; m++) {
-            const float f = c_lpf[color][m * 8 + l];
+            const float f = __ldg(&d_lpf[color][m * 8 + l]);
             cc[m] *= f; sc[m] *= f; cs[m] *= f; ss[m] *= f;
         }
     }

@@ -58,7 +58,7 @@ __device__ __forceinline__ void corr_job(const float *a, const float *b, int cst
         if (color == 1) { /* LPF after red and blue */
 #pragma unroll
             for (int m = 0; m < 8; m++) {
-                const float f = c_lpf[4][m * 8 + l];
+                const float f = __ldg(&d_lpf[4][m * 8 + l]);
 #pragma unroll
                 for (int q = 0; q < 4; q++) acc[q][m] *= f;
             }
@@ -71,7 +71,7 @@ __device__ __forceinline__ void corr_job(const float *a, const float *b, int cst
 #pragma unroll
         for (int q = 0; q < 4; q++) s2 = __fmaf_rn(acc[q][m], acc[q][m], s2);
         const float sc = rsqrtf(s2);
-        const float f = c_lpf[5][m * 8 + l];
+        const float f = __ldg(&d_lpf[5][m * 8 + l]);
 #pragma unroll
         for (int q = 0; q < 4; q++) acc[q][m] = (acc[q][m] * sc) * f;
     }

@@ -36,7 +36,6 @@ struct FrameParams {
     TextureParams tex; /* colors == 3, keep_weights == 0 */
 };
 
-constexpr int kCltJob = 264; /* floats per (camera, colour) CLT tile in shared memory; 264 % 32 == 8 */
 /* dynamic shared memory of k_frame, in floats */
 constexpr int kFrameSmemFloats = 12 * kCltJob + 12 * kJob + 12 * kJob + 12 * kTB4 + 4 * kCorrBuf + 16;
 constexpr size_t kFrameSmemBytes = sizeof(float) * kFrameSmemFloats;
@@ -47,7 +46,7 @@ __global__ void __launch_bounds__(128, 3) k_frame(
     const float *__restrict__ port_offsets, const int *__restrict__ woi, size_t rgba_stride,
     float *__restrict__ rgba, float *const *clt_out)
 {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     float *s_clt = smem;                      /* the tile's CLT, job = camera * 3 + colour */
     float *s_m = s_clt + 12 * kCltJob;        /* inverse-CLT tiles M                        */
     float *s_t = s_m + 12 * kJob;             /* un-windowed tiles T, then the RGBA slices  */
@@ -117,7 +116,7 @@ __global__ void __launch_bounds__(128, 3) k_frame(
         } else if (nbr) {
             const int cam = grp / 3, color = grp - cam * 3;
             float *mj = s_m + grp * kJob, *tj = s_t + grp * kJob, *xj = s_x + grp * kTB4;
-            imclt_unfold_job(s_clt + (cam * 3 + color) * kCltJob, c_lpf[color], xj, mj, tj, l, gm);
+            imclt_unfold_job(s_clt + (cam * 3 + color) * kCltJob, d_lpf[color], xj, mj, tj, l, gm);
             debayer_job(tj, xj, color < 2, p.tex.min_shot, p.tex.scale_shot, l, gm);
         }
         if (nbr) {
@@ -135,7 +134,7 @@ __global__ void __launch_bounds__(128, 3) k_frame(
             for (int e = tid; e < 4 * 256; e += 128) {
                 const int s = e >> 8, r = (e >> 4) & 15, c = e & 15;
                 float v = s_t[s * kJob + JT(r, c)];
-                if (nbr != TP_TASK_TEXTURE_BITS) v *= c_alpha_fade[nbr][r * 16 + c];
+                if (nbr != TP_TASK_TEXTURE_BITS) v *= __ldg(&d_alpha_fade[nbr][r * 16 + c]);
                 const long long gy = y0 + r, gx = x0 + c;
                 if (gy < 0 || gx < 0) continue;
                 float *pdst = rgba + (size_t)s * slice_stride + (size_t)gy * rgba_stride + (size_t)gx;

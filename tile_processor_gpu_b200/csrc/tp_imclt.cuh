@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(256) k_imclt_rbg(Geom g, const float *__restri
 #pragma unroll
         for (int hc = 0; hc < 2; hc++) {
             const int c = l + 8 * hc;
-            const float wc = 0.5f * c_hwin[c];
+            const float wc = 0.5f * __ldg(&d_hwin[c]);
             for (int r = 0; r < 16; r++) {
                 const float w = (0.5f * c_hwin[r]) * wc;
                 float *px = top + (size_t)r * dstride + c;

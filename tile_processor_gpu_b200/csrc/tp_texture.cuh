@@ -4,7 +4,10 @@
  * :3847-4017, debayer_shot / debayer :4019-4199 and tile_combine_rgba
  * :4202-4665).
  *
- * One 128-thread block per listed tile (grid-stride).  Per (camera, color)
+ * One 128-thread block per listed tile (grid-stride).  The block's next
+ * tile is staged one tile ahead with asynchronous copies: its CLT (into a
+ * bank-padded buffer, issued once the current CLT has been read) and, per
+ * thread, the RGBA pixels that thread will update.  Per (camera, color)
  * job one 8-lane group, working only with __syncwarp on its own buffers:
  *   1. low-pass filter and invert the CLT tile (vertical DCT-IV/DST-IV on the
  *      held column, transpose, horizontal pass on the held row) and unfold it
@@ -41,21 +44,19 @@ __device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
  * removed, T = M / (sin^2 r sin^2 c) = d / (4 sin r sin c), formed directly
  * from the signed sum d.  The quadrant signs of the unfold (idct_signs,
  * :399-420) factor into a vertical and a horizontal sign vector.  src: the
- * job's 4x64 coefficients (row stride 8), global or shared.  tout may be
+ * job's 4x64 coefficients (row stride 8) in shared memory.  tout may be
  * NULL (no debayer). */
 __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *mout,
                                                  float *tout, int l, unsigned gm)
 {
-    float in[4][8]; /* the job's 256 coefficients, column l of each quadrant */
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-#pragma unroll
-        for (int m = 0; m < 8; m++) in[q][m] = src[q * 64 + m * 8 + l];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         float col[8], v[8], row[8];
 #pragma unroll
-        for (int m = 0; m < 8; m++) col[m] = lpf ? in[q][m] * lpf[m * 8 + l] : in[q][m];
+        for (int m = 0; m < 8; m++) {
+            const float x = src[q * 64 + m * 8 + l];
+            col[m] = lpf ? x * __ldg(&lpf[m * 8 + l]) : x;
+        }
         if (q >> 1) dtt8<1>(col, v); else dtt8<0>(col, v);
 #pragma unroll
         for (int k = 0; k < 8; k++) tb[TBI(q, k, l)] = v[k];
@@ -78,7 +79,7 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
         const int cq = c >> 2;
         const float shc = (cq == 0) ? 1.0f : -1.0f; /* cosine horizontal */
         const float shs = (cq == 3) ? -1.0f : 1.0f; /* sine horizontal   */
-        const float hc = c_hwin[c];
+        const float hc = __ldg(&d_hwin[c]);
         const float wc = 0.5f * hc;
         const float tc = 0.25f / hc;
         const float *col = tb + v;
@@ -112,7 +113,7 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
         const int c = l + 8 * h;
         const bool cborder = (c == 0) || (c == 15);
         const int cm = cborder ? c : c - 1, cp = cborder ? c : c + 1;
-        const float hcc = c_hwin[c];
+        const float hcc = __ldg(&d_hwin[c]);
         const float wx = hcc * hcc;
         float a0 = t[JT(0, cm)], a1 = t[JT(0, c)], a2 = t[JT(0, cp)];
         float b0 = t[JT(1, cm)], b1 = t[JT(1, c)], b2 = t[JT(1, cp)];
@@ -270,6 +271,34 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
     for (int cam = 0; cam < 4; cam++) out[(COLORS + 1 + cam) * kJob + e] = pw[cam];
 }
 
+/* dynamic shared memory of k_textures, in floats: M, T/slices, transposes/D,
+ * the staged CLT of the tile, the prefetched RGBA pixels */
+constexpr int kTexSmemFloats = 12 * kJob + 12 * kJob + 12 * kTB4 + 12 * kCltJob + 4 * 256;
+constexpr size_t kTexSmemBytes = sizeof(float) * kTexSmemFloats;
+
+/* Stage the CLT of one tile (jobs cam * colors + color) into s_c with
+ * asynchronous copies: 16-byte chunks when every camera plane is 16-byte
+ * aligned, else 4-byte ones.  A camera plane holds the tile's three colours
+ * contiguously (768 floats). */
+__device__ __forceinline__ void stage_clt(float *const *cp, bool al16, int tile, int colors, float *s_c, int tid)
+{
+    if (al16 && colors == 3) {
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            const int k = tid + 128 * i; /* 16-byte chunk of the tile, 0..767 */
+            const int cam = k / 192, w = k - cam * 192;
+            cp_async16(s_c + (cam * 3 + (w >> 6)) * kCltJob + (w & 63) * 4, cp[cam] + (size_t)tile * 768 + w * 4);
+        }
+    } else {
+        const int njobs = 4 * colors;
+        for (int k = tid; k < njobs * 256; k += 128) {
+            const int job = k >> 8, e = k & 255;
+            const int cam = job / colors, color = job - cam * colors;
+            cp_async4(s_c + job * kCltJob + e, cp[cam] + ((size_t)tile * 3 + color) * 256 + e);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128, 3) k_textures(
     Geom g, const int *__restrict__ woi, float *const *clt, long long num_texture_tiles,
     const int *__restrict__ list, const int *__restrict__ dev_counts, int count_slot, int list_cap,
@@ -277,20 +306,36 @@ __global__ void __launch_bounds__(128, 3) k_textures(
     size_t texture_rbg_stride, float *__restrict__ texture_rbg, size_t texture_stride,
     float *__restrict__ texture_tiles)
 {
-    __shared__ float s_m[12 * kJob];   /* IMCLT tiles M (not debayered)                    */
-    __shared__ float s_d[12 * kJob];   /* un-windowed tiles T, then the output slices      */
-    __shared__ float s_x[12 * kTB4];   /* transposes, then the debayered tiles D           */
-    __shared__ float s_hsq[16], s_hsqi[16];
+    extern __shared__ __align__(16) float smem[];
+    float *s_m = smem;                 /* IMCLT tiles M (not debayered)                    */
+    float *s_d = s_m + 12 * kJob;      /* un-windowed tiles T, then the output slices      */
+    float *s_x = s_d + 12 * kJob;      /* transposes, then the debayered tiles D           */
+    float *s_c = s_x + 12 * kTB4;      /* the tile's CLT, staged one tile ahead            */
+    float *s_r = s_c + 12 * kCltJob;   /* RGBA pixels under the tile, prefetched per thread */
+    __shared__ float s_hsq[16];
+    __shared__ float *s_cp[4];
+    __shared__ float s_pd2r[6], s_chw[3];
 
     const int tid = threadIdx.x;
     const int l = tid & 7, grp = tid >> 3;
     const unsigned gm = group_mask();
     const int colors = p.colors;
     const int njobs = 4 * colors;
+    const float ksigma = (float)(1.0 / (2.0 * (double)p.diff_sigma * (double)p.diff_sigma));
     if (tid < 16) {
         const float s = c_hwin[tid];
         s_hsq[tid] = s * s;
-        s_hsqi[tid] = 1.0f / (s * s);
+    }
+    if (tid < 4) s_cp[tid] = clt[tid];
+    if (tid == 0) {
+        int k = 0;
+        for (int i = 0; i < 4; i++)
+            for (int j = i + 1; j < 4; j++) {
+                const float dx = port_offsets[2 * j] - port_offsets[2 * i];
+                const float dy = port_offsets[2 * j + 1] - port_offsets[2 * i + 1];
+                s_pd2r[k++] = ksigma / (dx * dx + dy * dy);
+            }
+        s_chw[0] = p.w0; s_chw[1] = p.w1; s_chw[2] = p.w2;
     }
 
     long long count = num_texture_tiles;
@@ -301,41 +346,92 @@ __global__ void __launch_bounds__(128, 3) k_textures(
         count = count < 0 ? 0 : (count > list_cap ? list_cap : count);
         if (border_quarter) lst = list + (border_quarter - count);
     }
+    const bool want_rbg = texture_rbg && texture_rbg_stride;
     int wx0 = 0, wy0 = 0, wh = 0;
-    if (texture_rbg && texture_rbg_stride) { wx0 = woi[0]; wy0 = woi[1]; wh = woi[3]; }
+    if (want_rbg) { wx0 = woi[0]; wy0 = woi[1]; wh = woi[3]; }
     const size_t slice_stride = texture_rbg_stride * (size_t)(wh + 1) * 8;
-    const float ksigma = (float)(1.0 / (2.0 * (double)p.diff_sigma * (double)p.diff_sigma));
-    float pd2r[6];
-    {
-        int k = 0;
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = i + 1; j < 4; j++) {
-                const float dx = port_offsets[2 * j] - port_offsets[2 * i];
-                const float dy = port_offsets[2 * j + 1] - port_offsets[2 * i + 1];
-                pd2r[k++] = ksigma / (dx * dx + dy * dy);
-            }
-    }
-    const float chw[3] = {p.w0, p.w1, p.w2};
     __syncthreads();
+    const bool al16 = !((reinterpret_cast<uintptr_t>(s_cp[0]) | reinterpret_cast<uintptr_t>(s_cp[1]) |
+                         reinterpret_cast<uintptr_t>(s_cp[2]) | reinterpret_cast<uintptr_t>(s_cp[3])) & 15);
+    const int ntiles = g.TX * g.TY;
+    /* list entry -> tile index, or -1 when the entry is not a texture tile */
+    auto tile_of = [&](long long n) -> int {
+        if (n >= count) return -1;
+        const int code = lst[n];
+        const int tile = code >> 8;
+        return ((code & (1 << 7)) && tile >= 0 && tile < ntiles) ? tile : -1;
+    };
+    /* Thread tid owns pixel (r0 + 8 (i & 1), c) of slice i >> 1 of the
+     * tile's 16x16 footprint in the RGBA image, element e = 128 i + tid of
+     * the slice buffers. */
+    const int own_c = tid & 15, own_r0 = tid >> 4;
+    const int own_n = 2 * (colors + 1);
+    /* address of the thread's first pixel under `tile`, or NULL when the
+     * footprint starts left of / above the window */
+    auto own_base = [&](int tile) -> float * {
+        const int ty = tile / g.TX, tx = tile - ty * g.TX;
+        const long long gy = (long long)(ty - wy0) * 8 + own_r0, gx = (long long)(tx - wx0) * 8 + own_c;
+        if (gy < 0 || gx < 0) return nullptr;
+        return texture_rbg + (size_t)gy * texture_rbg_stride + (size_t)gx;
+    };
+    /* prefetch the pixels this thread will update for list entry n; the same
+     * thread reads them back, so no barrier is needed */
+    auto stage_rgba = [&](long long n) {
+        if (!want_rbg || n >= count) return;
+        const int code = lst[n];
+        const int tile = code >> 8;
+        if (!(code & (1 << 7)) || tile < 0 || tile >= ntiles || !(code & TP_TASK_TEXTURE_BITS)) return;
+        float *b = own_base(tile);
+        if (!b) return;
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if (i < own_n)
+                cp_async4(s_r + i * 128 + tid, b + (size_t)(i >> 1) * slice_stride + (i & 1) * 8 * texture_rbg_stride);
+    };
+
+    {
+        const long long n0 = blockIdx.x;
+        const int t0 = tile_of(n0);
+        if (t0 >= 0) {
+            stage_clt(s_cp, al16, t0, colors, s_c, tid);
+            stage_rgba(n0);
+        }
+        cp_async_commit();
+    }
 
     for (long long n = blockIdx.x; n < count; n += gridDim.x) {
         const int code = lst[n];
-        const int tile = code >> 8;
-        if (!(code & (1 << 7)) || tile < 0 || tile >= g.TX * g.TY) continue;
+        const int tile = tile_of(n);
+        const long long n_next = n + gridDim.x;
+        cp_async_wait_all();
+        __syncthreads(); /* staged CLT visible; the previous tile's buffers free */
+        if (tile < 0) {
+            const int tn = tile_of(n_next);
+            if (tn >= 0) {
+                stage_clt(s_cp, al16, tn, colors, s_c, tid);
+                stage_rgba(n_next);
+            }
+            cp_async_commit();
+            continue;
+        }
 
         /* ---- stages 1-2: per (camera, color) group ---- */
         if (grp < njobs) {
             const int cam = grp / colors, color = grp - cam * colors;
-            const float *src = clt[cam] + ((size_t)tile * 3 + color) * 256;
             float *mj = s_m + grp * kJob, *tj = s_d + grp * kJob, *xj = s_x + grp * kTB4;
             /* M -> s_m; the un-windowed T -> s_d; the debayered D -> s_x
              * (the transpose buffer, free once the unfold has read it) */
-            imclt_unfold_job(src, c_lpf[colors > 1 ? color : 3], xj, mj, colors > 1 ? tj : nullptr, l, gm);
+            imclt_unfold_job(s_c + grp * kCltJob, d_lpf[colors > 1 ? color : 3], xj, mj, colors > 1 ? tj : nullptr,
+                             l, gm);
             if (colors > 1) debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
         }
         __syncthreads();
+        {
+            /* the CLT of this block's next tile lands while this one finishes */
+            const int tn = tile_of(n_next);
+            if (tn >= 0) stage_clt(s_cp, al16, tn, colors, s_c, tid);
+            cp_async_commit();
+        }
 
         /* ---- stage 3: fuse the four cameras, one thread per pixel; the
          * slices go to s_d ---- */
@@ -344,9 +440,11 @@ __global__ void __launch_bounds__(128, 3) k_textures(
             const int r = px >> 4, c = px & 15;
             const float wnd2 = s_hsq[sym8(r)] * s_hsq[sym8(c)];
             if (colors == 3)
-                combine_pixel<3>(s_x, kTB4, s_m, s_d, r, c, pd2r, ksigma, chw, wnd2, p.dust_remove, p.keep_weights);
+                combine_pixel<3>(s_x, kTB4, s_m, s_d, r, c, s_pd2r, ksigma, s_chw, wnd2, p.dust_remove,
+                                 p.keep_weights);
             else
-                combine_pixel<1>(s_m, kJob, s_m, s_d, r, c, pd2r, ksigma, chw, wnd2, p.dust_remove, p.keep_weights);
+                combine_pixel<1>(s_m, kJob, s_m, s_d, r, c, s_pd2r, ksigma, s_chw, wnd2, p.dust_remove,
+                                 p.keep_weights);
         }
         __syncthreads();
 
@@ -360,20 +458,19 @@ __global__ void __launch_bounds__(128, 3) k_textures(
             }
         }
         const int nbr = code & TP_TASK_TEXTURE_BITS;
-        if (texture_rbg && texture_rbg_stride && nbr) {
-            const int ty = tile / g.TX, tx = tile - ty * g.TX;
-            const long long x0 = (long long)(tx - wx0) * 8, y0 = (long long)(ty - wy0) * 8;
-            for (int e = tid; e < (colors + 1) * 256; e += 128) {
-                const int s = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                float v = s_d[s * kJob + JT(r, c)];
-                if (nbr != TP_TASK_TEXTURE_BITS) v *= c_alpha_fade[nbr][r * 16 + c];
-                const long long gy = y0 + r, gx = x0 + c;
-                if (gy < 0 || gx < 0) continue;
-                float *pdst = texture_rbg + (size_t)s * slice_stride + (size_t)gy * texture_rbg_stride + (size_t)gx;
-                *pdst += v;
+        float *b = (want_rbg && nbr) ? own_base(tile) : nullptr;
+        if (b) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                if (i >= own_n) break;
+                const int r = own_r0 + 8 * (i & 1);
+                float v = s_d[(i >> 1) * kJob + JT(r, own_c)];
+                if (nbr != TP_TASK_TEXTURE_BITS) v *= __ldg(&d_alpha_fade[nbr][r * 16 + own_c]);
+                b[(size_t)(i >> 1) * slice_stride + (i & 1) * 8 * texture_rbg_stride] = s_r[i * 128 + tid] + v;
             }
         }
-        __syncthreads();
+        stage_rgba(n_next);
+        cp_async_commit();
     }
 }
 
