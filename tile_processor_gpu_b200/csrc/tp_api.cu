@@ -229,8 +229,8 @@ int tp_textures_accumulate(const tp_geometry *g, const int *woi, float *const *c
     int sms;
     if ((rc = sm_count(&sms))) return rc;
     if ((rc = texture_smem_setup())) return rc;
-    unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, 3);
-    tp::k_textures<<<grid, 128, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
+    unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, 4);
+    tp::k_textures<<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
         gd, woi, clt, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
         want_tiles ? texture_tiles : nullptr);
@@ -343,13 +343,13 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
         tp::k_clear_rbga<<<grid, 256, 0, s>>>(woi, colors, 0, 0, texture_rbga_stride, texture_tiles);
     }
     const int quarter = gd.TX * (gd.TYA >> 2);
-    const unsigned grid = grid_for(quarter, 1, sms, 3);
+    const unsigned grid = grid_for(quarter, 1, sms, 4);
     if ((rc = texture_smem_setup())) return rc;
     for (int pass = 0; pass < 8; pass++) {
         const int border = pass >> 2;
         const int slot = ((pass & 3) << 1) + border;
         const int *base = texture_indices + (pass & 3) * quarter;
-        tp::k_textures<<<grid, 128, tp::kTexSmemBytes, s>>>(gd, woi, clt, 0, base, num_texture_tiles, slot, quarter,
+        tp::k_textures<<<grid, tp::kTexThreads, tp::kTexSmemBytes, s>>>(gd, woi, clt, 0, base, num_texture_tiles, slot, quarter,
                                             border ? quarter : 0, port_offsets, p, texture_rbga_stride,
                                             texture_tiles, 0, nullptr);
     }

@@ -4,22 +4,24 @@
  * :3847-4017, debayer_shot / debayer :4019-4199 and tile_combine_rgba
  * :4202-4665).
  *
- * One 128-thread block per listed tile (grid-stride).  The block's next
- * tile is staged one tile ahead with asynchronous copies: its CLT (into a
- * bank-padded buffer, issued once the current CLT has been read) and, per
- * thread, the RGBA pixels that thread will update.  Per (camera, color)
- * job one 8-lane group, working only with __syncwarp on its own buffers:
+ * One 96-thread block (three warps) per listed tile (grid-stride), four
+ * blocks per SM.  The block's next tile is staged one tile ahead with
+ * asynchronous copies: its CLT (into a bank-padded buffer, issued once the
+ * current CLT has been read) and, per thread, the RGBA pixels that thread
+ * will update.  Per (camera, color) job one 8-lane group, working only with
+ * __syncwarp on its own buffers:
  *   1. low-pass filter and invert the CLT tile (vertical DCT-IV/DST-IV on the
  *      held column, transpose, horizontal pass on the held row) and unfold it
- *      into the windowed 16x16 tile M and the un-windowed tile T;
+ *      into the un-windowed tile T (colour) or the windowed tile M (mono);
  *   2. debayer T with the 3x3 stencil (a register window walked down each
  *      column), apply the shot-noise square root and re-window into D (lane l
  *      owns columns l and l + 8).
- * After one block barrier every thread fuses the four cameras at two pixels
- * (stage 3), and the slices are written as non-overlapping 16x16 tiles and/or
- * faded by the neighbour mask and added into the overlapped RGBA image
- * (stage 4).  Per-job buffers are 280 floats apart (280 % 32 == 24) so the
- * four groups of a warp never share a bank.
+ * After one block barrier every thread fuses the four cameras at its pixels
+ * (stage 3; the plain windowed tile is T times the squared window) and
+ * writes them out itself (stage 4): as non-overlapping 16x16 tiles and/or
+ * faded by the neighbour mask and added into the overlapped RGBA image.
+ * Per-job buffers are 280 floats apart (280 % 32 == 24) so the four groups
+ * of a warp never share a bank.
  */
 #pragma once
 #include "tp_common.cuh"
@@ -44,8 +46,8 @@ __device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
  * removed, T = M / (sin^2 r sin^2 c) = d / (4 sin r sin c), formed directly
  * from the signed sum d.  The quadrant signs of the unfold (idct_signs,
  * :399-420) factor into a vertical and a horizontal sign vector.  src: the
- * job's 4x64 coefficients (row stride 8) in shared memory.  tout may be
- * NULL (no debayer). */
+ * job's 4x64 coefficients (row stride 8) in shared memory.  Either of mout
+ * and tout may be NULL. */
 __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *mout,
                                                  float *tout, int l, unsigned gm)
 {
@@ -93,7 +95,7 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
             const float d01 = (rq == 0) ? __fmaf_rn(shs, a1, shc * a0) : -__fmaf_rn(shs, a1, shc * a0);
             const float d23 = (rq == 3) ? -__fmaf_rn(shs, a3, shc * a2) : __fmaf_rn(shs, a3, shc * a2);
             const float d = d01 + d23;
-            mout[JT(r, c)] = ((0.5f * c_hwin[r]) * wc) * d;
+            if (mout) mout[JT(r, c)] = ((0.5f * c_hwin[r]) * wc) * d;
             if (tout) tout[JT(r, c)] = d * (tc / c_hwin[r]);
         }
     }
@@ -149,14 +151,16 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
 }
 
 /* Fuse the four cameras at one pixel (tile_combine_rgba, one pixel).
- * D: debayered, M: plain tiles, both [job = cam * colors + color].
- * Writes colors, alpha, 4 port weights and (keep_weights) colors+1 rms. */
+ * sd: debayered tiles D; sm: the plain (not debayered) tiles, scaled by
+ * m_scale (the plain tile is the un-windowed one times the squared window);
+ * both [job = cam * colors + color] with the given strides, pixel offset e.
+ * o: colours, alpha, 4 port weights and (keep_weights) colors + 1 rms. */
 template <int COLORS>
-__device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, const float *sm, float *out, int r,
-                                              int c, const float *pd2r, float ksigma, const float *chw, float wnd2,
-                                              int dust_remove, int keep_weights)
+__device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, const float *sm, int sm_stride,
+                                              float m_scale, int e, const float *pd2r, float ksigma,
+                                              const float *chw, float wnd2, int dust_remove, int keep_weights,
+                                              float *o)
 {
-    const int e = JT(r, c);
     float D[4][COLORS];
 #pragma unroll
     for (int cam = 0; cam < 4; cam++)
@@ -176,10 +180,10 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
                 ss = __fmaf_rn(dv, dv, ss);
             }
             const float mse = ss * 0.25f;
-            out[(COLORS + 5 + col) * kJob + e] = sqrtf(mse);
+            o[COLORS + 5 + col] = sqrtf(mse);
             sw = __fmaf_rn(chw[col], mse, sw);
         }
-        out[(COLORS + 5 + COLORS) * kJob + e] = sqrtf(sw);
+        o[COLORS + 5 + COLORS] = sqrtf(sw);
     }
     /* the reference forms 1/w, the weight floor and the dust-removal scale in
      * double; the float32 forms below give the correctly rounded reciprocal
@@ -263,17 +267,19 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
     for (int col = 0; col < COLORS; col++) {
         float v = 0.0f;
 #pragma unroll
-        for (int cam = 0; cam < 4; cam++) v = __fmaf_rn(kinv * pw[cam], sm[(cam * COLORS + col) * kJob + e], v);
-        out[col * kJob + e] = v;
+        for (int cam = 0; cam < 4; cam++) v = __fmaf_rn(kinv * pw[cam], sm[(cam * COLORS + col) * sm_stride + e], v);
+        o[col] = v * m_scale;
     }
-    out[COLORS * kJob + e] = wnd2 * ksum / 4.0f;
+    o[COLORS] = wnd2 * ksum / 4.0f;
 #pragma unroll
-    for (int cam = 0; cam < 4; cam++) out[(COLORS + 1 + cam) * kJob + e] = pw[cam];
+    for (int cam = 0; cam < 4; cam++) o[COLORS + 1 + cam] = pw[cam];
 }
 
-/* dynamic shared memory of k_textures, in floats: M, T/slices, transposes/D,
- * the staged CLT of the tile, the prefetched RGBA pixels */
-constexpr int kTexSmemFloats = 12 * kJob + 12 * kJob + 12 * kTB4 + 12 * kCltJob + 4 * 256;
+/* k_textures block: three warps, one 8-lane group per (camera, colour) job */
+constexpr int kTexThreads = 96;
+/* dynamic shared memory of k_textures, in floats: T (un-windowed tiles),
+ * transposes then D (debayered tiles), the staged CLT, the prefetched RGBA */
+constexpr int kTexSmemFloats = 12 * kJob + 12 * kTB4 + 12 * kCltJob + 4 * 256;
 constexpr size_t kTexSmemBytes = sizeof(float) * kTexSmemFloats;
 
 /* Stage the CLT of one tile (jobs cam * colors + color) into s_c with
@@ -284,14 +290,14 @@ __device__ __forceinline__ void stage_clt(float *const *cp, bool al16, int tile,
 {
     if (al16 && colors == 3) {
 #pragma unroll
-        for (int i = 0; i < 6; i++) {
-            const int k = tid + 128 * i; /* 16-byte chunk of the tile, 0..767 */
+        for (int i = 0; i < 768 / kTexThreads; i++) {
+            const int k = tid + kTexThreads * i; /* 16-byte chunk of the tile, 0..767 */
             const int cam = k / 192, w = k - cam * 192;
             cp_async16(s_c + (cam * 3 + (w >> 6)) * kCltJob + (w & 63) * 4, cp[cam] + (size_t)tile * 768 + w * 4);
         }
     } else {
         const int njobs = 4 * colors;
-        for (int k = tid; k < njobs * 256; k += 128) {
+        for (int k = tid; k < njobs * 256; k += kTexThreads) {
             const int job = k >> 8, e = k & 255;
             const int cam = job / colors, color = job - cam * colors;
             cp_async4(s_c + job * kCltJob + e, cp[cam] + ((size_t)tile * 3 + color) * 256 + e);
@@ -299,7 +305,7 @@ __device__ __forceinline__ void stage_clt(float *const *cp, bool al16, int tile,
     }
 }
 
-__global__ void __launch_bounds__(128, 3) k_textures(
+__global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     Geom g, const int *__restrict__ woi, float *const *clt, long long num_texture_tiles,
     const int *__restrict__ list, const int *__restrict__ dev_counts, int count_slot, int list_cap,
     int border_quarter, const float *__restrict__ port_offsets, TextureParams p,
@@ -307,11 +313,10 @@ __global__ void __launch_bounds__(128, 3) k_textures(
     float *__restrict__ texture_tiles)
 {
     extern __shared__ __align__(16) float smem[];
-    float *s_m = smem;                 /* IMCLT tiles M (not debayered)                    */
-    float *s_d = s_m + 12 * kJob;      /* un-windowed tiles T, then the output slices      */
-    float *s_x = s_d + 12 * kJob;      /* transposes, then the debayered tiles D           */
-    float *s_c = s_x + 12 * kTB4;      /* the tile's CLT, staged one tile ahead            */
-    float *s_r = s_c + 12 * kCltJob;   /* RGBA pixels under the tile, prefetched per thread */
+    float *s_t = smem;                 /* un-windowed tiles T (colour) or windowed M (mono) */
+    float *s_x = s_t + 12 * kJob;      /* transposes, then the debayered tiles D            */
+    float *s_c = s_x + 12 * kTB4;      /* the tile's CLT, staged one tile ahead             */
+    float *s_r = s_c + 12 * kCltJob;   /* RGBA pixels under the tile, [slice][256]          */
     __shared__ float s_hsq[16];
     __shared__ float *s_cp[4];
     __shared__ float s_pd2r[6], s_chw[3];
@@ -347,6 +352,8 @@ __global__ void __launch_bounds__(128, 3) k_textures(
         if (border_quarter) lst = list + (border_quarter - count);
     }
     const bool want_rbg = texture_rbg && texture_rbg_stride;
+    const bool want_tiles = texture_tiles && texture_stride;
+    const int ns_tiles = (colors == 3) ? (p.keep_weights ? 12 : 4) : (p.keep_weights ? 8 : 2);
     int wx0 = 0, wy0 = 0, wh = 0;
     if (want_rbg) { wx0 = woi[0]; wy0 = woi[1]; wh = woi[3]; }
     const size_t slice_stride = texture_rbg_stride * (size_t)(wh + 1) * 8;
@@ -361,32 +368,28 @@ __global__ void __launch_bounds__(128, 3) k_textures(
         const int tile = code >> 8;
         return ((code & (1 << 7)) && tile >= 0 && tile < ntiles) ? tile : -1;
     };
-    /* Thread tid owns pixel (r0 + 8 (i & 1), c) of slice i >> 1 of the
-     * tile's 16x16 footprint in the RGBA image, element e = 128 i + tid of
-     * the slice buffers. */
-    const int own_c = tid & 15, own_r0 = tid >> 4;
-    const int own_n = 2 * (colors + 1);
-    /* address of the thread's first pixel under `tile`, or NULL when the
-     * footprint starts left of / above the window */
-    auto own_base = [&](int tile) -> float * {
+    /* RGBA address of pixel px (slice 0) under `tile`, or NULL when it lies
+     * left of / above the window */
+    auto rgba_at = [&](int tile, int px) -> float * {
         const int ty = tile / g.TX, tx = tile - ty * g.TX;
-        const long long gy = (long long)(ty - wy0) * 8 + own_r0, gx = (long long)(tx - wx0) * 8 + own_c;
+        const long long gy = (long long)(ty - wy0) * 8 + (px >> 4), gx = (long long)(tx - wx0) * 8 + (px & 15);
         if (gy < 0 || gx < 0) return nullptr;
         return texture_rbg + (size_t)gy * texture_rbg_stride + (size_t)gx;
     };
-    /* prefetch the pixels this thread will update for list entry n; the same
-     * thread reads them back, so no barrier is needed */
+    /* Thread tid combines pixels tid, tid + 96, tid + 192 (< 256) and owns
+     * them in the RGBA image: it prefetches them for list entry n and reads
+     * them back itself, so no barrier is needed. */
     auto stage_rgba = [&](long long n) {
         if (!want_rbg || n >= count) return;
         const int code = lst[n];
         const int tile = code >> 8;
         if (!(code & (1 << 7)) || tile < 0 || tile >= ntiles || !(code & TP_TASK_TEXTURE_BITS)) return;
-        float *b = own_base(tile);
-        if (!b) return;
 #pragma unroll
-        for (int i = 0; i < 8; i++)
-            if (i < own_n)
-                cp_async4(s_r + i * 128 + tid, b + (size_t)(i >> 1) * slice_stride + (i & 1) * 8 * texture_rbg_stride);
+        for (int px = tid; px < 256; px += kTexThreads) {
+            const float *b = rgba_at(tile, px);
+            if (!b) continue;
+            for (int sl = 0; sl <= colors; sl++) cp_async4(s_r + sl * 256 + px, b + (size_t)sl * slice_stride);
+        }
     };
 
     {
@@ -418,12 +421,15 @@ __global__ void __launch_bounds__(128, 3) k_textures(
         /* ---- stages 1-2: per (camera, color) group ---- */
         if (grp < njobs) {
             const int cam = grp / colors, color = grp - cam * colors;
-            float *mj = s_m + grp * kJob, *tj = s_d + grp * kJob, *xj = s_x + grp * kTB4;
-            /* M -> s_m; the un-windowed T -> s_d; the debayered D -> s_x
-             * (the transpose buffer, free once the unfold has read it) */
-            imclt_unfold_job(s_c + grp * kCltJob, d_lpf[colors > 1 ? color : 3], xj, mj, colors > 1 ? tj : nullptr,
-                             l, gm);
-            if (colors > 1) debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
+            float *tj = s_t + grp * kJob, *xj = s_x + grp * kTB4;
+            if (colors > 1) {
+                /* T -> s_t, then the debayered D -> s_x (the transpose
+                 * buffer, free once the unfold has read it) */
+                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[color], xj, nullptr, tj, l, gm);
+                debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
+            } else {
+                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[3], xj, tj, nullptr, l, gm);
+            }
         }
         __syncthreads();
         {
@@ -433,40 +439,38 @@ __global__ void __launch_bounds__(128, 3) k_textures(
             cp_async_commit();
         }
 
-        /* ---- stage 3: fuse the four cameras, one thread per pixel; the
-         * slices go to s_d ---- */
-#pragma unroll 1
-        for (int px = tid; px < 256; px += 128) {
-            const int r = px >> 4, c = px & 15;
-            const float wnd2 = s_hsq[sym8(r)] * s_hsq[sym8(c)];
-            if (colors == 3)
-                combine_pixel<3>(s_x, kTB4, s_m, s_d, r, c, s_pd2r, ksigma, s_chw, wnd2, p.dust_remove,
-                                 p.keep_weights);
-            else
-                combine_pixel<1>(s_m, kJob, s_m, s_d, r, c, s_pd2r, ksigma, s_chw, wnd2, p.dust_remove,
-                                 p.keep_weights);
-        }
-        __syncthreads();
-
-        /* ---- stage 4: outputs ---- */
-        if (texture_tiles && texture_stride) {
-            const int ns = (colors == 3) ? (p.keep_weights ? 12 : 4) : (p.keep_weights ? 8 : 2);
-            float *dst = texture_tiles + (size_t)n * texture_stride;
-            for (int e = tid; e < ns * 256; e += 128) {
-                const int s = e >> 8, r = (e >> 4) & 15, c = e & 15;
-                dst[e] = s_d[s * kJob + JT(r, c)];
-            }
-        }
+        /* ---- stages 3-4: fuse the four cameras at the thread's pixels and
+         * write them out ---- */
         const int nbr = code & TP_TASK_TEXTURE_BITS;
-        float *b = (want_rbg && nbr) ? own_base(tile) : nullptr;
-        if (b) {
+#pragma unroll 1
+        for (int px = tid; px < 256; px += kTexThreads) {
+            const int r = px >> 4, c = px & 15;
+            const int e = JT(r, c);
+            const float wnd2 = s_hsq[sym8(r)] * s_hsq[sym8(c)];
+            float o[12];
+            if (colors == 3)
+                combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, wnd2, p.dust_remove,
+                                 p.keep_weights, o);
+            else
+                combine_pixel<1>(s_t, kJob, s_t, kJob, 1.0f, e, s_pd2r, ksigma, s_chw, wnd2, p.dust_remove,
+                                 p.keep_weights, o);
+            if (want_tiles) {
+                float *dst = texture_tiles + (size_t)n * texture_stride + px;
 #pragma unroll
-            for (int i = 0; i < 8; i++) {
-                if (i >= own_n) break;
-                const int r = own_r0 + 8 * (i & 1);
-                float v = s_d[(i >> 1) * kJob + JT(r, own_c)];
-                if (nbr != TP_TASK_TEXTURE_BITS) v *= __ldg(&d_alpha_fade[nbr][r * 16 + own_c]);
-                b[(size_t)(i >> 1) * slice_stride + (i & 1) * 8 * texture_rbg_stride] = s_r[i * 128 + tid] + v;
+                for (int sl = 0; sl < 12; sl++)
+                    if (sl < ns_tiles) dst[sl * 256] = o[sl];
+            }
+            if (want_rbg && nbr) {
+                float *b = rgba_at(tile, px);
+                if (b) {
+                    const float f = (nbr != TP_TASK_TEXTURE_BITS) ? __ldg(&d_alpha_fade[nbr][px]) : 1.0f;
+#pragma unroll
+                    for (int sl = 0; sl < 4; sl++) {
+                        if (sl > colors) break;
+                        const float v = (nbr != TP_TASK_TEXTURE_BITS) ? o[sl] * f : o[sl];
+                        b[(size_t)sl * slice_stride] = s_r[sl * 256 + px] + v;
+                    }
+                }
             }
         }
         stage_rgba(n_next);
