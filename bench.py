@@ -39,6 +39,7 @@ WIDTH, HEIGHT = 2592, 1936
 METRIC = "quad 5MP frames/s (CLT+corr+texture)"
 UNIT = "frames/s"
 CORR_RADIUS = 7
+DISPARITY_ERROR = 0.5
 FAT_ZERO = 0.05
 TEXTURE = dict(colors=3, is_lwir=0, min_shot=10.0, scale_shot=3.0, diff_sigma=1.5, diff_threshold=10.0,
                min_agree=3.0, weight0=0.294118, weight1=0.117647, weight2=0.588235, dust_remove=1, keep_weights=0)
@@ -50,9 +51,10 @@ WORKLOAD = ("full-frame quad 2592x1936 Bayer (78,408 tiles): forward CLT + aberr
 FLOPS_PER_TILE = {"convert": 75776, "correlate": 92016, "texture": 149304}
 # FP32 SIMT: 148 SMs x 128 lanes x 2 flop x 1.965 GHz
 FP32_NOMINAL_TFLOPS = 74.4
-# DRAM bytes per launch-set of each stage from an ncu capture of this workload
-# (dram__bytes_read.sum + dram__bytes_write.sum summed over the stage's kernels)
-TRAFFIC = {}
+# DRAM bytes of each stage of one frame of this workload from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum summed over the stage's
+# launches; profiles/launch_list_2592x1936_quad.md)
+TRAFFIC = {"convert": 1384.7e6, "correlate": 1358.9e6, "texture": 1555.7e6}
 
 
 def peaks():
@@ -163,13 +165,19 @@ class FramePipeline:
         self.geom_d = synth.geometry(WIDTH, HEIGHT, image_rows=HEIGHT + 16)
         g = self.g = api.Geometry.from_dict(self.geom_d)
         self.TX, self.TY, self.TYA = synth.tiles(self.geom_d)
-        imgs, disp = synth.plane_scene(rng, WIDTH, HEIGHT, disparity=(0.0, 64.0))
+        imgs, disp = synth.plane_scene(rng, WIDTH, HEIGHT, disparity=(0.0, 64.0), texture="detail")
         self.dstride = WIDTH + 64
         pitched = np.zeros((4, HEIGHT + 16, self.dstride), np.float32)
         pitched[:, :HEIGHT, :WIDTH] = imgs
         self.host_images = [torch.from_numpy(pitched[c]).pin_memory() for c in range(4)]
-        kern, extra = synth.kernel_tables(rng, self.geom_d, pool=256)
-        self.tasks_np = synth.tasks_grid(self.geom_d, rng, jitter=0.5, disparity=disp)
+        # centred PSFs without kernel-centre offsets: the cameras carry no
+        # shift the scene does not have, so the disparity is measurable
+        kern, extra = synth.kernel_tables(rng, self.geom_d, pool=256, zero_extra=True, psf_offset=0.0)
+        # tasks at the true disparity plus a per-tile error U[-0.5, 0.5] px:
+        # the residual the correlations measure is minus that error
+        self.tasks_np, err = synth.tasks_grid(self.geom_d, rng, jitter=0.0, disparity=disp,
+                                              disparity_error=DISPARITY_ERROR, return_error=True)
+        self.true_residual = -err
         self.num_tiles = int(self.tasks_np.size)
         self.images = [h.to(device) for h in self.host_images]
         self.kernels = [torch.from_numpy(kern[c]).to(device) for c in range(4)]
@@ -193,6 +201,8 @@ class FramePipeline:
         self.rgba_rows = (self.TY + 1) * 8 * (TEXTURE["colors"] + 1)
         self.rgba = torch.empty((self.rgba_rows, self.rgba_stride), dtype=torch.float32, device=device)
         self.port_offsets = torch.from_numpy(synth.PORT_OFFSETS.reshape(-1).copy()).to(device)
+        self.disparity = torch.empty(self.TX * self.TY, dtype=torch.float32, device=device)
+        self.strength = torch.empty(self.TX * self.TY, dtype=torch.float32, device=device)
         # kernel-table bytes a frame touches (distinct kernel tiles of all jobs)
         self.kernel_tiles_touched = self._touched_kernel_tiles()
         self.host_corrs = torch.empty_like(self.corrs, device="cpu").pin_memory()
@@ -234,6 +244,26 @@ class FramePipeline:
                                min_shot=t["min_shot"], scale_shot=t["scale_shot"], diff_sigma=t["diff_sigma"],
                                weight0=t["weight0"], weight1=t["weight1"], weight2=t["weight2"],
                                dust_remove=t["dust_remove"])
+
+    def disparity_fit(self):
+        self.api.disparity_fit(self.g, self.corrs, self.corr_stride, CORR_RADIUS, self.num_corr, self.corr_idx,
+                               self.port_offsets, self.disparity, self.strength)
+
+    def disparity_accuracy(self):
+        """RMS error of the fitted residual against the truth on tiles whose
+        footprint stays inside every camera's frame (disparity <= 64 px moves
+        a camera by <= 32 px: 5 tiles of margin)"""
+        tx = self.tasks_np["txy"] & 0xFFFF
+        ty = self.tasks_np["txy"] >> 16
+        inner = (tx >= 5) & (tx < self.TX - 5) & (ty >= 5) & (ty < self.TY - 5)
+        got = self.disparity.cpu().numpy()[ty * self.TX + tx].astype(np.float64)
+        res = got[inner] - self.true_residual[inner]
+        return {"rmse_px": round(float(np.sqrt(np.mean(res ** 2))), 4),
+                "outliers_gt_0.5px": round(float(np.mean(np.abs(res) > 0.5)), 5),
+                "truth_rms_px": round(float(np.sqrt(np.mean(self.true_residual[inner] ** 2))), 4),
+                "tiles": int(inner.sum()), "fit": "3-point parabola on the 6-pair profile (tp_disparity_fit mode 0)",
+                "truth": "plane scene disparity; task error U[-%.1f, %.1f] px per tile" % (DISPARITY_ERROR,
+                                                                                        DISPARITY_ERROR)}
 
     STAGES = ("convert", "correlate", "texture")
     LAUNCHES = {"convert": 1, "correlate": 1, "texture": 15}
@@ -311,6 +341,21 @@ def run_b200(args, rank, world, local, pg):
     torch.cuda.synchronize()
     fused_ms = f0.elapsed_time(f1) / fused_steps
 
+    # the disparity fit on the frame's correlations (the consumer of stage 2)
+    pipe.step()
+    pipe.disparity_fit()
+    torch.cuda.synchronize()
+    d0 = torch.cuda.Event(enable_timing=True)
+    d1 = torch.cuda.Event(enable_timing=True)
+    d0.record(stream)
+    for _ in range(fused_steps):
+        pipe.disparity_fit()
+    d1.record(stream)
+    torch.cuda.synchronize()
+    fit_ms = d0.elapsed_time(d1) / fused_steps
+    disparity = pipe.disparity_accuracy()
+    disparity["fit_ms"] = round(fit_ms, 4)
+
     # ---- end to end through the public API with host buffers ----
     e2e_steps = max(2, min(args.steps, 10))
     h2d = sum(h.numel() * 4 for h in pipe.host_images)
@@ -342,16 +387,17 @@ def run_b200(args, rank, world, local, pg):
     out = {
         "metric": METRIC, "value": round(fps, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plane scene, PSF kernels)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plane scene, centred PSF kernels)",
         "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "tiles": pipe.num_tiles,
                    "corr_tiles": pipe.num_corr, "parallelism": "frame replicas x%d" % world,
                    "path": "tp_convert_correct_tiles + tp_correlate2D + tp_generate_RBGA",
                    "l2": "per-step working set %.2f GB > 126 MB L2 (no flush)" % (sum(algo.values()) / 1e9)},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "fused_frame_ms": round(fused_ms, 4),
+        "disparity": disparity,
         "roofline": {"bound": "hbm", "kernel": "k_textures (%s stage)" % dom, "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
-                     "algorithmic_bytes": int(algo[dom]), "traffic": TRAFFIC.get(dom),
+                     "algorithmic_bytes": int(algo[dom]), "traffic": int(TRAFFIC[dom]) if dom in TRAFFIC else None,
                      "fp32_simt": {"flops": int(flops), "achieved_tflops": round(flops / (stage_ms[dom] * 1e-3) / 1e12, 2),
                                    "nominal_peak_tflops": FP32_NOMINAL_TFLOPS}},
         "e2e": {"value": round(world / (e2e_ms * 1e-3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -379,12 +425,12 @@ def cpu_pipeline(sample_tiles, seed=0):
     w = WIDTH
     h = max(32, min(HEIGHT, (sample_tiles // (WIDTH // 8)) * 8))
     geom = synth.geometry(w, h, image_rows=h + 16)
-    imgs, disp = synth.plane_scene(rng, w, h, disparity=(0.0, 64.0))
+    imgs, disp = synth.plane_scene(rng, w, h, disparity=(0.0, 64.0), texture="detail")
     dstride = w + 64
     pitched = np.zeros((4, h + 16, dstride), np.float32)
     pitched[:, :h, :w] = imgs
-    kern, extra = synth.kernel_tables(rng, geom, pool=256)
-    tasks = synth.tasks_grid(geom, rng, jitter=0.5, disparity=disp)
+    kern, extra = synth.kernel_tables(rng, geom, pool=256, zero_extra=True, psf_offset=0.0)
+    tasks = synth.tasks_grid(geom, rng, jitter=0.0, disparity=disp, disparity_error=DISPARITY_ERROR)
     corr_idx = synth.corr_indices_fast(tasks, geom)
     TX, TY, _ = synth.tiles(geom)
 
@@ -427,7 +473,7 @@ def run_reference(args, rank, world, pg):
     return {
         "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 / v, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded plane scene, PSF kernels)",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded plane scene, centred PSF kernels)",
         "impl": "reference",
         "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT),
                    "sample_tiles_per_step": ntiles, "parallelism": "host threads"},

@@ -265,6 +265,29 @@ int tp_process_frame(const tp_geometry *g,
                      float *const *clt,
                      tp_stream_t stream);
 
+/* ---- disparity from the pair correlations ---------------------------------------
+ * No counterpart in the reference, which hands its correlation tiles to the
+ * Java caller (src/TileProcessor.cuh:1176-1443 is where it stops).  For each
+ * tile with listed pairs (entries of one tile adjacent in corr_indices, as
+ * the correlation lists are built), the profile
+ *   S(k) = sum over its pairs p in pair_mask of C_p(k * b_p),  k = -r..r,
+ * b_p = port_offsets[j] - port_offsets[i] for pair p = (i, j), C_p sampled
+ * bilinearly in the centred (2r+1)^2 tile, is maximised to sub-pixel precision
+ * (double precision) around its first integer maximum:
+ *   mode 0: 3-point parabola; 1: 5-point least-squares parabola; 2: 3-point
+ *   centroid; the sub-pixel step stays within +-1.
+ * disparity[tile] = the residual disparity rho (true minus task disparity, in
+ * pixels per unit of port offset: pair p peaks at rho * b_p); strength[tile]
+ * = the fitted peak per pair.  Both are device float[tilesx * tilesy], written
+ * only for fitted tiles.  corrs / corr_stride / corr_radius / corr_indices
+ * as tp_correlate2D's output. */
+int tp_disparity_fit(const tp_geometry *g,
+                     const float *corrs, size_t corr_stride, int corr_radius,
+                     size_t num_corr_tiles, const int *corr_indices,
+                     const float *port_offsets, int pair_mask, int mode,
+                     float *disparity, float *strength,
+                     tp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

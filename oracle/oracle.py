@@ -182,3 +182,29 @@ def generate_RBGA(geom, tasks, width, height, clt, port_offsets, texture_rbga_st
                             ctypes.c_int(0), ctypes.c_size_t(texture_rbga_stride), _p(out), ctypes.c_size_t(rows),
                             _p(lp))
     return out, t, idx, counts, woi
+
+
+def disparity_fit(geom, corrs, corr_indices, corr_radius=7, port_offsets=None, pair_mask=0x3F, mode=0):
+    """Residual disparity and strength per tile (NaN where not fitted)."""
+    TX, TY = geom["img_width"] // 8, geom["img_height"] // 8
+    c = np.ascontiguousarray(corrs, dtype=np.float32)
+    idx = np.ascontiguousarray(corr_indices, dtype=np.int32)
+    if port_offsets is None:
+        port_offsets = np.array([[-0.5, -0.5], [0.5, -0.5], [-0.5, 0.5], [0.5, 0.5]], dtype=np.float32)
+    po = np.ascontiguousarray(port_offsets, dtype=np.float32).reshape(8)
+    disp = np.full(TX * TY, np.nan)
+    strength = np.full(TX * TY, np.nan)
+    lib().tpo_disparity_fit(ctypes.byref(_g(geom)), _p(c), ctypes.c_size_t(c.shape[1]), ctypes.c_int(corr_radius),
+                            ctypes.c_int(idx.size), _p(idx), _p(po), ctypes.c_int(pair_mask), ctypes.c_int(mode),
+                            _p(disp), _p(strength))
+    return disp, strength
+
+
+def fit_profile(S, valid=None, mode=0):
+    S = np.ascontiguousarray(S, dtype=np.float64)
+    v = np.ones(S.size, dtype=np.int32) if valid is None else np.ascontiguousarray(valid, dtype=np.int32)
+    rho = ctypes.c_double()
+    pk = ctypes.c_double()
+    lib().tpo_fit_profile(_p(S), _p(v), ctypes.c_int((S.size - 1) // 2), ctypes.c_int(mode), ctypes.byref(rho),
+                          ctypes.byref(pk))
+    return rho.value, pk.value

@@ -852,3 +852,135 @@ int tpo_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *
     }
     return 0;
 }
+
+/* ---- disparity from the pair correlations (new: the reference leaves this
+ * step to its Java caller; this is the method the library implements) ----
+ *
+ * Pair p = (i, j) of a tile correlates at its peak at rho * b_p, with
+ * b_p = port_offsets[j] - port_offsets[i] and rho the residual disparity
+ * (true minus task disparity).  The tile's profile is
+ *   S(k) = sum over its listed pairs in pair_mask of C_p(k * b_p),
+ * k = -r..r, C_p sampled bilinearly in the centred (2r+1)^2 tile; a k whose
+ * sample of any contributing pair leaves the tile is not used.  rho is the
+ * sub-pixel maximum of S around its first integer argmax k*:
+ *   mode 0: parabola through S(k*-1), S(k*), S(k*+1);
+ *   mode 1: least-squares parabola through the valid S(k*-2 .. k*+2);
+ *   mode 2: centroid of S - min over k*-1 .. k*+1.
+ * The sub-pixel offset is kept within [-1, 1]; a fit without a maximum gives
+ * k*.  strength = the fitted peak value / number of pairs. */
+static int fit_sample(const float *c, int r, double x, double y, double *out)
+{
+    const double fx0 = floor(x), fy0 = floor(y);
+    const int ix = (int)fx0, iy = (int)fy0;
+    const double fx = x - fx0, fy = y - fy0;
+    const int n = 2 * r + 1;
+    if (ix < -r || iy < -r || ix > r || iy > r) return 0;
+    if ((fx > 0.0 && ix + 1 > r) || (fy > 0.0 && iy + 1 > r)) return 0;
+    double v = (1.0 - fx) * (1.0 - fy) * c[(iy + r) * n + ix + r];
+    if (fx > 0.0) v += fx * (1.0 - fy) * c[(iy + r) * n + ix + 1 + r];
+    if (fy > 0.0) v += (1.0 - fx) * fy * c[(iy + 1 + r) * n + ix + r];
+    if (fx > 0.0 && fy > 0.0) v += fx * fy * c[(iy + 1 + r) * n + ix + 1 + r];
+    *out = v;
+    return 1;
+}
+
+void tpo_fit_profile(const double *S, const int *valid, int r, int mode, double *rho, double *peak)
+{
+    const int n = 2 * r + 1;
+    int km = -1;
+    for (int k = 0; k < n; k++)
+        if (valid[k] && (km < 0 || S[k] > S[km])) km = k;
+    if (km < 0) { *rho = NAN; *peak = 0.0; return; }
+    double off = 0.0, pk = S[km];
+    if (mode == 0) {
+        if (km > 0 && km < n - 1 && valid[km - 1] && valid[km + 1]) {
+            const double a = S[km - 1], b = S[km], c = S[km + 1];
+            const double den = a - 2.0 * b + c;
+            if (den < 0.0) {
+                off = 0.5 * (a - c) / den;
+                if (off > 1.0) off = 1.0;
+                if (off < -1.0) off = -1.0;
+                pk = b - 0.25 * (a - c) * off;
+            }
+        }
+    } else if (mode == 1) {
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, y0 = 0, y1 = 0, y2 = 0;
+        int cnt = 0;
+        for (int t = -2; t <= 2; t++) {
+            const int k = km + t;
+            if (k < 0 || k >= n || !valid[k]) continue;
+            const double tt = t, y = S[k];
+            s0 += 1; s1 += tt; s2 += tt * tt; s3 += tt * tt * tt; s4 += tt * tt * tt * tt;
+            y0 += y; y1 += tt * y; y2 += tt * tt * y;
+            cnt++;
+        }
+        if (cnt >= 3) {
+            /* normal equations [s0 s1 s2; s1 s2 s3; s2 s3 s4] [a b c] = [y0 y1 y2] */
+            const double det = s0 * (s2 * s4 - s3 * s3) - s1 * (s1 * s4 - s3 * s2) + s2 * (s1 * s3 - s2 * s2);
+            if (det != 0.0) {
+                const double a = (y0 * (s2 * s4 - s3 * s3) - s1 * (y1 * s4 - s3 * y2) + s2 * (y1 * s3 - s2 * y2)) / det;
+                const double b = (s0 * (y1 * s4 - y2 * s3) - y0 * (s1 * s4 - s3 * s2) + s2 * (s1 * y2 - y1 * s2)) / det;
+                const double c = (s0 * (s2 * y2 - s3 * y1) - s1 * (s1 * y2 - s3 * y0) + y0 * (s1 * s3 - s2 * s2)) / det;
+                if (c < 0.0) {
+                    off = -b / (2.0 * c);
+                    if (off > 1.0) off = 1.0;
+                    if (off < -1.0) off = -1.0;
+                    pk = a + b * off + c * off * off;
+                }
+            }
+        }
+    } else {
+        if (km > 0 && km < n - 1 && valid[km - 1] && valid[km + 1]) {
+            const double a = S[km - 1], b = S[km], c = S[km + 1];
+            const double m = fmin(a, fmin(b, c));
+            const double w = (a - m) + (b - m) + (c - m);
+            if (w > 0.0) off = ((c - m) - (a - m)) / w;
+        }
+    }
+    *rho = (km - r) + off;
+    *peak = pk;
+}
+
+int tpo_disparity_fit(const tp_geometry *g, const float *corrs, size_t corr_stride, int corr_radius,
+                      int num_corr_tiles, const int *corr_indices, const float *port_offsets, int pair_mask,
+                      int mode, double *disparity, double *strength)
+{
+    init_tables();
+    const int r = corr_radius, n = 2 * r + 1;
+    const int ntiles = tiles_x(g) * tiles_y(g);
+    double bx[6], by[6];
+    for (int p = 0; p < 6; p++) {
+        const int i = PAIRS[p][0], j = PAIRS[p][1];
+        bx[p] = (double)port_offsets[2 * j] - (double)port_offsets[2 * i];
+        by[p] = (double)port_offsets[2 * j + 1] - (double)port_offsets[2 * i + 1];
+    }
+    int done = 0;
+    for (int e = 0; e < num_corr_tiles; e++) {
+        const int tile = corr_indices[e] >> 8;
+        if (e > 0 && (corr_indices[e - 1] >> 8) == tile) continue; /* not the start of the tile's run */
+        if (tile < 0 || tile >= ntiles) continue;
+        double S[2 * TP_MAX_CORR_RADIUS + 1];
+        int valid[2 * TP_MAX_CORR_RADIUS + 1];
+        int npairs = 0;
+        for (int k = 0; k < n; k++) { S[k] = 0.0; valid[k] = 1; }
+        for (int e2 = e; e2 < num_corr_tiles && (corr_indices[e2] >> 8) == tile; e2++) {
+            const int p = corr_indices[e2] & 0xff;
+            if (p > 5 || !((pair_mask >> p) & 1)) continue;
+            npairs++;
+            for (int k = 0; k < n; k++) {
+                double v;
+                if (fit_sample(corrs + (size_t)e2 * corr_stride, r, (k - r) * bx[p], (k - r) * by[p], &v))
+                    S[k] += v;
+                else
+                    valid[k] = 0;
+            }
+        }
+        if (!npairs) continue;
+        double rho, pk;
+        tpo_fit_profile(S, valid, r, mode, &rho, &pk);
+        disparity[tile] = rho;
+        strength[tile] = pk / npairs;
+        done++;
+    }
+    return done;
+}

@@ -101,6 +101,19 @@ int tpo_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles,
                       size_t texture_rbga_rows,
                       const float *lpf);
 
+/* Disparity fit from the pair correlations (new: the reference leaves it
+ * to its Java caller).  Entries of one tile must be adjacent in
+ * corr_indices.  disparity / strength: double[tilesx * tilesy], written for
+ * tiles with at least one listed pair in pair_mask (residual disparity, in
+ * pixels per unit of port offset, and the fitted peak per pair).
+ * mode 0: 3-point parabola, 1: 5-point least-squares parabola, 2: 3-point
+ * centroid.  Returns the number of tiles fitted. */
+int tpo_disparity_fit(const tp_geometry *g, const float *corrs, size_t corr_stride, int corr_radius,
+                      int num_corr_tiles, const int *corr_indices, const float *port_offsets, int pair_mask,
+                      int mode, double *disparity, double *strength);
+/* the sub-pixel step alone, on a profile S[2r+1] with validity flags */
+void tpo_fit_profile(const double *S, const int *valid, int r, int mode, double *rho, double *peak);
+
 /* Window tables: 0 = exact (default), 1 = rounded to 6 decimals like the
  * reference's printed tables (used to find outputs sensitive to them). */
 void tpo_set_table_mode(int mode);

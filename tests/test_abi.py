@@ -93,6 +93,15 @@ def test_rejects_bad_arguments(native):
     # generate_RBGA stride below (tilesx + 1) * 8
     assert _code(lambda: N.call("tp_generate_RBGA", g.ptr, fake, 4, fake, fake, fake, 32, 32, fake, fake, *args, 0,
                                 263, fake, None)) == N.TP_ERR_ARG
+    # disparity fit: radius above 7, mode 3, stride below (2r+1)^2, NULL output
+    assert _code(lambda: N.call("tp_disparity_fit", g.ptr, fake, 225, 8, 4, fake, fake, 63, 0, fake, fake,
+                                None)) == N.TP_ERR_ARG
+    assert _code(lambda: N.call("tp_disparity_fit", g.ptr, fake, 225, 7, 4, fake, fake, 63, 3, fake, fake,
+                                None)) == N.TP_ERR_ARG
+    assert _code(lambda: N.call("tp_disparity_fit", g.ptr, fake, 200, 7, 4, fake, fake, 63, 0, fake, fake,
+                                None)) == N.TP_ERR_ARG
+    assert _code(lambda: N.call("tp_disparity_fit", g.ptr, fake, 225, 7, 4, fake, fake, 63, 0, None, fake,
+                                None)) == N.TP_ERR_ARG
     # LPF table index
     v = np.zeros(64, np.float32)
     assert _code(lambda: N.call("tp_set_lpf", 6, v.ctypes.data_as(P))) == N.TP_ERR_ARG
@@ -106,5 +115,6 @@ def test_zero_work_is_ok_without_gpu(native):
     fake = P(0x1000)
     assert N.call("tp_correlate2D", g.ptr, fake, 3, 1., 1., 1., .1, 0, None, 225, 7, None, None) == 0
     assert N.call("tp_convert_correct_tiles", g.ptr, fake, fake, fake, None, fake, 256, 0, 0, None) == 0
+    assert N.call("tp_disparity_fit", g.ptr, None, 225, 7, 0, None, None, 63, 0, None, None, None) == 0
     assert N.call("tp_textures_accumulate", g.ptr, None, fake, 0, None, None, 3, 0, 10., 3., 1.5, 10., 3., .3, .1, .6, 1,
                   0, 0, None, 0, None, None) == 0

@@ -60,6 +60,7 @@ SIGNATURES = {
                          _I, _S, _P, _P],
     "tp_process_frame": [_G, _P, _P, _P, _S, _P, _I, _I, _I, _F, _F, _F, _F, _I, _S, _P, _P, _F, _F, _F, _F, _F,
                          _F, _I, _P, _P, _P, _S, _P, _P, _P],
+    "tp_disparity_fit": [_G, _P, _S, _I, _S, _P, _P, _I, _I, _P, _P, _P],
     "tp_set_lpf": [_I, _P],
     "tp_get_lpf": [_I, _P],
     "tp_reset_lpf": [],

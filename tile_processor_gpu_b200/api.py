@@ -183,6 +183,15 @@ def process_frame(geom, gpu_kernel_offsets, gpu_kernels, gpu_images, dstride, gp
                  _stream(stream))
 
 
+def disparity_fit(geom, gpu_corrs, corr_stride, corr_radius, num_corr_tiles, gpu_corr_indices, gpu_port_offsets,
+                  gpu_disparity, gpu_strength, pair_mask=0x3F, mode=0, stream=None):
+    """Residual disparity and strength per tile from the pair correlations
+    (written into gpu_disparity / gpu_strength, float[tilesx * tilesy])."""
+    _native.call("tp_disparity_fit", geom.ptr, _dptr(gpu_corrs), int(corr_stride), int(corr_radius),
+                 int(num_corr_tiles), _dptr(gpu_corr_indices), _dptr(gpu_port_offsets), int(pair_mask), int(mode),
+                 _dptr(gpu_disparity), _dptr(gpu_strength), _stream(stream))
+
+
 def set_lpf(which, values):
     """Replace a low-pass table on the current device (0..3 lpf_data, 4 lpf_rb_corr, 5 lpf_corr)."""
     a = np.ascontiguousarray(values, dtype=np.float32).reshape(64)

@@ -18,6 +18,7 @@
 #include "tp_imclt.cuh"
 #include "tp_list.cuh"
 #include "tp_frame.cuh"
+#include "tp_disparity.cuh"
 
 #define TP_VERSION "tile_processor_gpu_b200 0.1 (sm_100a)"
 
@@ -414,6 +415,30 @@ int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *
         tp::k_frame<<<grid, 128, tp::kFrameSmemBytes, s>>>(gd, dstride, kernel_offsets, kernels, images, tasks, num_tiles, parity, fp,
                                          corrs, port_offsets, woi, texture_rbga_stride, texture_rbga, clt);
     return cuda_status(cudaGetLastError(), "process_frame launch");
+}
+
+int tp_disparity_fit(const tp_geometry *g, const float *corrs, size_t corr_stride, int corr_radius,
+                     size_t num_corr_tiles, const int *corr_indices, const float *port_offsets, int pair_mask,
+                     int mode, float *disparity, float *strength, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (corr_radius < 0 || corr_radius > TP_MAX_CORR_RADIUS)
+        return fail(TP_ERR_ARG, "corr_radius %d outside 0..%d", corr_radius, TP_MAX_CORR_RADIUS);
+    const size_t sz = (size_t)(2 * corr_radius + 1) * (2 * corr_radius + 1);
+    if (mode < 0 || mode > 2) return fail(TP_ERR_ARG, "mode %d (0, 1 or 2)", mode);
+    if (num_corr_tiles == 0) return TP_OK;
+    if (!corrs || !corr_indices || !port_offsets || !disparity || !strength)
+        return fail(TP_ERR_ARG, "NULL corrs / corr_indices / port_offsets / disparity / strength");
+    if (corr_stride < sz) return fail(TP_ERR_ARG, "corr_stride %zu < (2r+1)^2 = %zu", corr_stride, sz);
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    const unsigned grid = grid_for((long long)num_corr_tiles, 8, sms, 8);
+    tp::k_disparity_fit<<<grid, 256, 0, (cudaStream_t)stream>>>(gd.TX * gd.TY, corrs, corr_stride, corr_radius,
+                                                               (long long)num_corr_tiles, corr_indices,
+                                                               port_offsets, pair_mask, mode, disparity, strength);
+    return cuda_status(cudaGetLastError(), "disparity_fit launch");
 }
 
 } /* extern "C" */

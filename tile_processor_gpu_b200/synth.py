@@ -80,31 +80,42 @@ def smooth_bayer(rng, width, height, cams=4):
     return np.stack([smooth_noise(rng, height, width).astype(np.float32) for _ in range(cams)])
 
 
+# texture octaves of plane_scene: (scale px, weight); 'smooth' is dominated by
+# 48-px structure, 'detail' adds strong 4-px and 2-px octaves (fine texture
+# that correlation can lock onto under the shot noise)
+TEXTURES = {"smooth": ((48, 12, 3), (1.0, 0.6, 0.35)), "detail": ((24, 8, 4, 2), (0.6, 0.8, 1.0, 1.0))}
+
+
 def plane_scene(rng, width, height, disparity=(0.0, 64.0), port_offsets=PORT_OFFSETS, gain=0.01,
-                read_sigma=0.002, peak=1.0):
+                read_sigma=0.002, peak=1.0, texture="smooth"):
     """Quad-camera Bayer frame of a random-texture slanted plane.
 
-    The plane has disparity d(x, y) = d0 + gx x + gy y spanning `disparity`;
-    camera k sees scene point p at pixel p + d * port_offsets[k] (so a tile
-    centred at c in the scene is centred at c + d(c) * port_offsets[k] in
-    camera k, as tasks_grid places it).  Poisson-Gaussian
-    noise: v + sqrt(gain v) N + read_sigma N.  Returns (images [4][H][W],
-    disparity function coefficients (d0, gx, gy)).
+    The plane has disparity d(s) = d0 + gx sx + gy sy (s in scene
+    coordinates) spanning `disparity`; camera k sees scene point s at pixel
+    p = s + d(s) o_k, o_k = port_offsets[k] (so a tile centred at c in the
+    scene is centred at c + d(c) o_k in camera k, exactly as tasks_grid
+    places it).  Each camera pixel p is rendered from the scene point
+    s = q - o_k (g . q) / (1 + g . o_k), q = p - d0 o_k, g = (gx, gy), the
+    inverse of that map.  Poisson-Gaussian noise: v + sqrt(gain v) N +
+    read_sigma N.  Returns (images [4][H][W], disparity function coefficients
+    (d0, gx, gy)).
     """
     H, W = height, width
-    tex = np.stack([smooth_noise(rng, H + 96, W + 96, scales=(48, 12, 3), weights=(1.0, 0.6, 0.35))
-                    for _ in range(3)])
+    scales, weights = TEXTURES[texture]
+    tex = np.stack([smooth_noise(rng, H + 96, W + 96, scales=scales, weights=weights) for _ in range(3)])
     dlo, dhi = disparity
     gx = (dhi - dlo) * rng.uniform(0.3, 0.7) / W
     gy = (dhi - dlo - gx * W) / H
     d0 = dlo
     cmap = bayer_color_map(H, W)
     yy, xx = np.mgrid[0:H, 0:W].astype(np.float64)
-    d = d0 + gx * xx + gy * yy
     imgs = []
     for k in range(len(port_offsets)):
-        sx = xx - d * port_offsets[k][0] + 48.0
-        sy = yy - d * port_offsets[k][1] + 48.0
+        ox, oy = float(port_offsets[k][0]), float(port_offsets[k][1])
+        qx, qy = xx - d0 * ox, yy - d0 * oy
+        gq = (gx * qx + gy * qy) / (1.0 + gx * ox + gy * oy)
+        sx = qx - ox * gq + 48.0
+        sy = qy - oy * gq + 48.0
         x0 = np.clip(np.floor(sx).astype(np.int64), 0, W + 94); fx = sx - x0
         y0 = np.clip(np.floor(sy).astype(np.int64), 0, H + 94); fy = sy - y0
         t = tex[cmap, y0, x0] * (1 - fx) * (1 - fy) + tex[cmap, y0, x0 + 1] * fx * (1 - fy) + \
@@ -154,11 +165,14 @@ def psf_to_clt(h):
     return out
 
 
-def kernel_tables(rng, geom, kind="gauss", pool=256, zero_extra=False, cams=4):
+def kernel_tables(rng, geom, kind="gauss", pool=256, zero_extra=False, cams=4, psf_offset=0.25):
     """CLT kernel tables and CltExtra tables for every camera.
 
-    kind 'gauss': seeded anisotropic Gaussian PSFs (sigma 0.5..1.5 px) drawn
-    from a pool of `pool` shapes; 'identity': CC = 1, other quadrants 0.
+    kind 'gauss': seeded anisotropic Gaussian PSFs (sigma 0.5..1.5 px, centre
+    within +-psf_offset px) drawn from a pool of `pool` shapes; 'identity':
+    CC = 1, other quadrants 0.  Random kernel-centre offsets and Jacobians
+    unless zero_extra.  Centred PSFs with zero_extra shift no camera, so the
+    scene's disparity is measured without bias.
     Returns (kernels [cams][kv*kh*3*256], extra [cams][kv*kh*3*8]) float32.
     """
     kh, kv = geom["kernels_hor"], geom["kernels_vert"]
@@ -167,7 +181,7 @@ def kernel_tables(rng, geom, kind="gauss", pool=256, zero_extra=False, cams=4):
         k = np.zeros((cams, nk, 4, 8, 8), dtype=np.float32)
         k[:, :, 0] = 1.0
     else:
-        clt_pool = psf_to_clt(_psf_pool(rng, pool)).astype(np.float32)
+        clt_pool = psf_to_clt(_psf_pool(rng, pool, offset=psf_offset)).astype(np.float32)
         pick = rng.integers(0, pool, size=(cams, nk))
         k = clt_pool[pick]
     extra = np.zeros((cams, nk, 8), dtype=np.float32)
@@ -185,12 +199,14 @@ def kernel_tables(rng, geom, kind="gauss", pool=256, zero_extra=False, cams=4):
 
 
 def tasks_grid(geom, rng=None, jitter=0.5, task_bits=ALL_TASK_BITS, disparity=None,
-               port_offsets=PORT_OFFSETS, mask=None):
+               port_offsets=PORT_OFFSETS, mask=None, disparity_error=0.0, return_error=False):
     """One task per tile in raster order (tiles with mask False are left out).
 
     xy[cam] = tile centre (8 tx + 4, 8 ty + 4) + U[-jitter, jitter] per
-    camera + d(tx, ty) * port_offsets[cam] when `disparity` = (d0, gx, gy),
-    rounded to 1/256 px."""
+    camera + (d(tx, ty) + e) * port_offsets[cam] when `disparity` = (d0, gx,
+    gy), rounded to 1/256 px; e = U[-disparity_error, disparity_error] per
+    tile, the same for all cameras (the task's disparity error, so the tile's
+    residual disparity is -e).  With return_error, returns (tasks, e)."""
     TX, TY, _ = tiles(geom)
     ty, tx = np.meshgrid(np.arange(TY), np.arange(TX), indexing="ij")
     tx = tx.reshape(-1); ty = ty.reshape(-1)
@@ -203,6 +219,9 @@ def tasks_grid(geom, rng=None, jitter=0.5, task_bits=ALL_TASK_BITS, disparity=No
     t["txy"] = tx + (ty << 16)
     cx = (tx * 8 + 4).astype(np.float64)
     cy = (ty * 8 + 4).astype(np.float64)
+    err = np.zeros(n)
+    if disparity_error and rng is not None:
+        err = rng.uniform(-disparity_error, disparity_error, n)
     for cam in range(4):
         x, y = cx.copy(), cy.copy()
         if rng is not None and jitter:
@@ -210,12 +229,12 @@ def tasks_grid(geom, rng=None, jitter=0.5, task_bits=ALL_TASK_BITS, disparity=No
             y += rng.uniform(-jitter, jitter, n)
         if disparity is not None:
             d0, gx, gy = disparity
-            d = d0 + gx * cx + gy * cy
+            d = d0 + gx * cx + gy * cy + err
             x += d * port_offsets[cam][0]
             y += d * port_offsets[cam][1]
         t["xy"][:, cam, 0] = np.round(x * 256.0) / 256.0
         t["xy"][:, cam, 1] = np.round(y * 256.0) / 256.0
-    return t
+    return (t, err) if return_error else t
 
 
 def corr_indices(tasks, geom):
