@@ -513,3 +513,21 @@ def test_process_frame_matches_stage_kernels(frames, name):
     assert np.array_equal(woi_np, woi_ref)
     h, w = _rgba_region(woi_np)
     assert rel_err(rgba.cpu().numpy()[:4 * h, :w], rgba_ref[:4 * h, :w]) < 1e-6
+
+
+@pytest.mark.parametrize("width,height,stride", [(256, 40, 272), (264, 17, 270), (2600, 31, 2600), (96, 8, 103)])
+def test_clear_texture_rbga_extent(native, width, height, stride):
+    """clear_texture_rbga zeroes `height` rows of the reference's column
+    extent -- the width plus the 8 floats its last thread writes past it
+    when the grid reaches that far, within the stride -- and nothing else."""
+    import torch
+    from tile_processor_gpu_b200 import api
+    g = api.Geometry(256, 256)
+    buf = torch.full((height + 3, stride), 3.0, device="cuda")
+    api.clear_texture_rbga(g, width, height, stride, buf)
+    torch.cuda.synchronize()
+    b = buf.cpu().numpy()
+    cols = min(width + 8, (width + 255) // 256 * 256, stride)
+    assert np.all(b[:height, :cols] == 0.0)
+    assert np.all(b[:height, cols:] == 3.0)
+    assert np.all(b[height:] == 3.0)

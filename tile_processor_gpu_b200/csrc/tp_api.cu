@@ -308,9 +308,10 @@ int tp_clear_texture_rbga(const tp_geometry *g, int texture_width, int texture_s
     if (texture_width < 0 || texture_slice_height < 0) return fail(TP_ERR_ARG, "negative extent");
     if (texture_rbga_stride < (size_t)texture_width) return fail(TP_ERR_ARG, "stride < width");
     if (texture_width == 0 || texture_slice_height == 0) return TP_OK;
-    dim3 grid((unsigned)((texture_width + 8 + 255) / 256), (unsigned)(texture_slice_height < 65535 ? texture_slice_height : 65535), 1);
-    tp::k_clear_rbga<<<grid, 256, 0, (cudaStream_t)stream>>>(nullptr, 0, texture_width, texture_slice_height,
-                                                             texture_rbga_stride, texture_tiles);
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    tp::k_clear_rbga<<<grid_for(texture_slice_height, 1, sms, 16), 256, 0, (cudaStream_t)stream>>>(
+        nullptr, 0, texture_width, texture_slice_height, texture_rbga_stride, texture_tiles);
     return cuda_status(cudaGetLastError(), "clear_texture_rbga launch");
 }
 
@@ -340,8 +341,8 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
     if ((rc = sm_count(&sms))) return rc;
     {
         const int max_rows = (gd.TY + 1) * 8 * (colors + 1);
-        dim3 grid((unsigned)(((gd.TX + 2) * 8 + 255) / 256), (unsigned)(max_rows < 65535 ? max_rows : 65535), 1);
-        tp::k_clear_rbga<<<grid, 256, 0, s>>>(woi, colors, 0, 0, texture_rbga_stride, texture_tiles);
+        tp::k_clear_rbga<<<grid_for(max_rows, 1, sms, 16), 256, 0, s>>>(woi, colors, 0, 0, texture_rbga_stride,
+                                                                         texture_tiles);
     }
     const int quarter = gd.TX * (gd.TYA >> 2);
     const unsigned grid = grid_for(quarter, 1, sms, 4);
@@ -391,8 +392,8 @@ int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *
     if ((rc = sm_count(&sms))) return rc;
     {
         const int max_rows = (gd.TY + 1) * 8 * 4;
-        dim3 grid((unsigned)(((gd.TX + 2) * 8 + 255) / 256), (unsigned)(max_rows < 65535 ? max_rows : 65535), 1);
-        tp::k_clear_rbga<<<grid, 256, 0, s>>>(woi, 3, 0, 0, texture_rbga_stride, texture_rbga);
+        tp::k_clear_rbga<<<grid_for(max_rows, 1, sms, 16), 256, 0, s>>>(woi, 3, 0, 0, texture_rbga_stride,
+                                                                         texture_rbga);
     }
     tp::FrameParams fp;
     fp.lpf_mask = lpf_mask;

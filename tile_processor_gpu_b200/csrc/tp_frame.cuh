@@ -37,7 +37,7 @@ struct FrameParams {
 };
 
 /* dynamic shared memory of k_frame, in floats */
-constexpr int kFrameSmemFloats = 12 * kCltJob + 12 * kJob + 12 * kJob + 12 * kTB4 + 4 * kCorrBuf + 16;
+constexpr int kFrameSmemFloats = 12 * kCltJob + 12 * kJob + 12 * kJob + 12 * kTB4 + 4 * kCorrBuf + 16 + 2 * kFac;
 constexpr size_t kFrameSmemBytes = sizeof(float) * kFrameSmemFloats;
 
 __global__ void __launch_bounds__(128, 3) k_frame(
@@ -53,10 +53,12 @@ __global__ void __launch_bounds__(128, 3) k_frame(
     float *s_x = s_t + 12 * kJob;             /* transposes, then the debayered tiles D     */
     float *s_corr = s_x + 12 * kTB4;          /* warp 3's correlation buffers               */
     float *s_hsq = s_corr + 4 * kCorrBuf;
+    float *s_tfac = s_hsq + 16, *s_mfac = s_tfac + kFac;
 
     const int tid = threadIdx.x;
     const int l = tid & 7, grp = tid >> 3;
     const unsigned gm = group_mask();
+    fill_unfold_factors(s_tfac, s_mfac, tid, 128);
     if (tid < 16) {
         const float s = c_hwin[tid];
         s_hsq[tid] = s * s;
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(128, 3) k_frame(
         } else if (nbr) {
             const int cam = grp / 3, color = grp - cam * 3;
             float *mj = s_m + grp * kJob, *tj = s_t + grp * kJob, *xj = s_x + grp * kTB4;
-            imclt_unfold_job(s_clt + (cam * 3 + color) * kCltJob, d_lpf[color], xj, mj, tj, l, gm);
+            imclt_unfold_job(s_clt + (cam * 3 + color) * kCltJob, d_lpf[color], xj, mj, tj, s_tfac, s_mfac, l, gm);
             debayer_job(tj, xj, color < 2, p.tex.min_shot, p.tex.scale_shot, l, gm);
         }
         if (nbr) {

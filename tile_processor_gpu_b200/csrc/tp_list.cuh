@@ -129,10 +129,15 @@ __global__ void k_clear_rbga(const int *woi, int colors, int texture_width, int 
     long long cols = (long long)tw + 8;
     if (cols > reach) cols = reach;
     if (cols > (long long)stride) cols = (long long)stride;
-    for (long long row = blockIdx.y; row < rows; row += gridDim.y) {
+    /* one block per row (grid-stride); 16-byte stores when every row starts
+     * on a 16-byte boundary, the last cols % 4 floats one by one */
+    const bool vec = !(reinterpret_cast<uintptr_t>(buf) & 15) && !(stride & 3);
+    const long long quads = vec ? cols >> 2 : 0;
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
         float *p = buf + (size_t)row * stride;
-        for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += (long long)gridDim.x * blockDim.x)
-            p[c] = 0.0f;
+        float4 *p4 = reinterpret_cast<float4 *>(p);
+        for (long long q = threadIdx.x; q < quads; q += blockDim.x) p4[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (long long c = quads * 4 + threadIdx.x; c < cols; c += blockDim.x) p[c] = 0.0f;
     }
 }
 

@@ -40,17 +40,38 @@ constexpr int kJob = 280;        /* floats per 16x17 job tile, padded */
 
 __device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
 
+/* Per-pixel factors of the unfold, [16][17] (row stride 17: the eight lanes
+ * of a group read eight rows of one column from distinct banks):
+ *   tfac[r][c] = (0.25 / w[c]) / w[r]     un-windowed tile T = d * tfac
+ *   mfac[r][c] = (0.5 w[r]) (0.5 w[c])    windowed tile M = mfac * d
+ * with w the half-sine window, in the rounding order of the per-pixel form. */
+constexpr int kFac = 16 * 17;
+__device__ __forceinline__ void fill_unfold_factors(float *tfac, float *mfac, int tid, int nthreads)
+{
+    for (int i = tid; i < 256; i += nthreads) {
+        const int r = i >> 4, c = i & 15;
+        const float hr = c_hwin[r], hc = c_hwin[c];
+        tfac[r * 17 + c] = (0.25f / hc) / hr;
+        mfac[r * 17 + c] = (0.5f * hr) * (0.5f * hc);
+    }
+}
+
 /* Windowed inverse CLT of one job (imclt8threads, :3847-4017) into the
  * [16][17] tile M = w * d (w the product of the two half-sine windows, no
  * accumulation), and, for the debayer, the same tile with the squared window
  * removed, T = M / (sin^2 r sin^2 c) = d / (4 sin r sin c), formed directly
- * from the signed sum d.  The quadrant signs of the unfold (idct_signs,
- * :399-420) factor into a vertical and a horizontal sign vector.  src: the
- * job's 4x64 coefficients (row stride 8) in shared memory.  Either of mout
- * and tout may be NULL. */
+ * from the signed sum d.  Lane l ends the two passes holding pixel-domain row
+ * l of all four quadrants in registers; the unfold (fold row RIND[r] = l for
+ * exactly two output rows r) then writes those two rows whole, the quadrant
+ * signs of idct_signs (:399-420) factored into a vertical sign per row and a
+ * horizontal sign per column.  src: the job's 4x64 coefficients (row stride
+ * 8) in shared memory; tb: the group's transpose buffer.  Either of mout and
+ * tout may be NULL (with its factor table). */
 __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *mout,
-                                                 float *tout, int l, unsigned gm)
+                                                 float *tout, const float *tfac, const float *mfac, int l,
+                                                 unsigned gm)
 {
+    float a[4][8]; /* pixel-domain row l of each quadrant */
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         float col[8], v[8], row[8];
@@ -65,38 +86,28 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
         __syncwarp(gm);
 #pragma unroll
         for (int k = 0; k < 8; k++) row[k] = tb[TBI(q, l, k)];
-        __syncwarp(gm);
-        if (q & 1) dtt8<1>(row, v); else dtt8<0>(row, v);
-        /* pixel-domain row l of quadrant q replaces its transpose buffer */
-#pragma unroll
-        for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
+        if (q & 1) dtt8<1>(row, a[q]); else dtt8<0>(row, a[q]);
     }
-    __syncwarp(gm);
-    /* unfold: output row r reads fold row RIND[r]; lane l writes columns l
-     * and l + 8 of every row */
+    /* the two output rows folding onto row l, and their vertical signs
+     * (rows 0-3: +,+; 4-7: -,+; 8-11: -,+; 12-15: -,-) */
 #pragma unroll 1
     for (int h = 0; h < 2; h++) {
-        const int c = l + 8 * h;
-        const int v = (c < 4) ? c + 4 : (c < 12) ? 11 - c : c - 12;
-        const int cq = c >> 2;
-        const float shc = (cq == 0) ? 1.0f : -1.0f; /* cosine horizontal */
-        const float shs = (cq == 3) ? -1.0f : 1.0f; /* sine horizontal   */
-        const float hc = __ldg(&d_hwin[c]);
-        const float wc = 0.5f * hc;
-        const float tc = 0.25f / hc;
-        const float *col = tb + v;
+        const int r = (l >= 4) ? (h ? 11 - l : l - 4) : (h ? l + 12 : 11 - l);
+        const int rq = r >> 2;
+        const bool n01 = rq != 0, n23 = rq == 3;
 #pragma unroll
-        for (int r = 0; r < 16; r++) {
-            const int u = (r < 4) ? r + 4 : (r < 12) ? 11 - r : r - 12;
-            const int rq = r >> 2;
-            const float a0 = col[TBI(0, u, 0)], a1 = col[TBI(1, u, 0)];
-            const float a2 = col[TBI(2, u, 0)], a3 = col[TBI(3, u, 0)];
-            /* (+/-shc) a0 + (+/-shs) a1 with the vertical sign known here */
-            const float d01 = (rq == 0) ? __fmaf_rn(shs, a1, shc * a0) : -__fmaf_rn(shs, a1, shc * a0);
-            const float d23 = (rq == 3) ? -__fmaf_rn(shs, a3, shc * a2) : __fmaf_rn(shs, a3, shc * a2);
-            const float d = d01 + d23;
-            if (mout) mout[JT(r, c)] = ((0.5f * c_hwin[r]) * wc) * d;
-            if (tout) tout[JT(r, c)] = d * (tc / c_hwin[r]);
+        for (int c = 0; c < 16; c++) {
+            const int v = (c < 4) ? c + 4 : (c < 12) ? 11 - c : c - 12;
+            const int cq = c >> 2;
+            /* (shc a0 + shs a1), (shc a2 + shs a3): shc = + for columns 0-3,
+             * shs = - for columns 12-15 */
+            const float e0 = (cq == 0) ? ((cq == 3) ? a[0][v] - a[1][v] : a[0][v] + a[1][v])
+                                       : ((cq == 3) ? -a[0][v] - a[1][v] : a[1][v] - a[0][v]);
+            const float e1 = (cq == 0) ? ((cq == 3) ? a[2][v] - a[3][v] : a[2][v] + a[3][v])
+                                       : ((cq == 3) ? -a[2][v] - a[3][v] : a[3][v] - a[2][v]);
+            const float d = (n01 ? -e0 : e0) + (n23 ? -e1 : e1);
+            if (mout) mout[JT(r, c)] = mfac[r * 17 + c] * d;
+            if (tout) tout[JT(r, c)] = d * tfac[r * 17 + c];
         }
     }
 }
@@ -320,6 +331,7 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     __shared__ float s_hsq[16];
     __shared__ float *s_cp[4];
     __shared__ float s_pd2r[6], s_chw[3];
+    __shared__ float s_tfac[kFac], s_mfac[kFac];
 
     const int tid = threadIdx.x;
     const int l = tid & 7, grp = tid >> 3;
@@ -327,6 +339,7 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     const int colors = p.colors;
     const int njobs = 4 * colors;
     const float ksigma = (float)(1.0 / (2.0 * (double)p.diff_sigma * (double)p.diff_sigma));
+    fill_unfold_factors(s_tfac, s_mfac, tid, kTexThreads);
     if (tid < 16) {
         const float s = c_hwin[tid];
         s_hsq[tid] = s * s;
@@ -425,10 +438,10 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
             if (colors > 1) {
                 /* T -> s_t, then the debayered D -> s_x (the transpose
                  * buffer, free once the unfold has read it) */
-                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[color], xj, nullptr, tj, l, gm);
+                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[color], xj, nullptr, tj, s_tfac, nullptr, l, gm);
                 debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
             } else {
-                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[3], xj, tj, nullptr, l, gm);
+                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[3], xj, tj, nullptr, nullptr, s_mfac, l, gm);
             }
         }
         __syncthreads();
