@@ -129,8 +129,8 @@ __global__ void __launch_bounds__(128, 3) k_frame(
                 const int r = px >> 4, c = px & 15;
                 const float wnd2 = s_hsq[sym8(r)] * s_hsq[sym8(c)];
                 float o[12];
-                combine_pixel<3>(s_x, kTB4, s_m, kJob, 1.0f, JT(r, c), pd2r, ksigma, chw, wnd2, p.tex.dust_remove,
-                                 0, o);
+                combine_pixel<3>(s_x, kTB4, s_m, kJob, 1.0f, JT(r, c), pd2r, ksigma, chw, wnd2, __frcp_rn(wnd2),
+                                 p.tex.dust_remove, 0, o);
 #pragma unroll
                 for (int sl = 0; sl < 4; sl++) s_t[sl * kJob + JT(r, c)] = o[sl];
             }

@@ -169,8 +169,8 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
 template <int COLORS>
 __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, const float *sm, int sm_stride,
                                               float m_scale, int e, const float *pd2r, float ksigma,
-                                              const float *chw, float wnd2, int dust_remove, int keep_weights,
-                                              float *o)
+                                              const float *chw, float wnd2, float wi, int dust_remove,
+                                              int keep_weights, float *o)
 {
     float D[4][COLORS];
 #pragma unroll
@@ -196,10 +196,10 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
         }
         o[COLORS + 5 + COLORS] = sqrtf(sw);
     }
-    /* the reference forms 1/w, the weight floor and the dust-removal scale in
-     * double; the float32 forms below give the correctly rounded reciprocal
-     * and round the floor sum once (at most one ulp from the double path) */
-    const float wi = __frcp_rn(wnd2);
+    /* wi = 1 / wnd2 correctly rounded (the reference forms it in double).
+     * The weights use the hardware exponential: its relative error (below
+     * 1e-6 wherever a weight is above the 1e-4 floor) is under what float32
+     * inputs already move them by. */
     float pw[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     {
         int k = 0;
@@ -213,7 +213,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
                     const float dc = (D[i][col] - D[j][col]) * wi;
                     d = __fmaf_rn(chw[col] * dc, dc, d);
                 }
-                const float x = expf(-pd2r[k] * d) + 1e-4f;
+                const float x = __expf(-pd2r[k] * d) + 1e-4f;
                 pw[i] += x;
                 pw[j] += x;
                 k++;
@@ -231,7 +231,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
         if (cam == b1) p1 = pw[cam];
         if (cam == b2) p2 = pw[cam];
     }
-    const float w1 = p1 / (p1 + p2);
+    const float w1 = __fdividef(p1, p1 + p2);
     const float w2 = 1.0f - w1;
     float avg[COLORS];
 #pragma unroll
@@ -252,7 +252,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
             const float dc = (D[cam][col] - avg[col]) * wi;
             d2 = __fmaf_rn(chw[col] * dc, dc, d2);
         }
-        pw[cam] = expf(-ksigma * d2) + 1e-4f;
+        pw[cam] = __expf(-ksigma * d2) + 1e-4f;
     }
     if (dust_remove) {
         int worst = 0;
@@ -264,9 +264,10 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
         float a = -wv;
 #pragma unroll
         for (int cam = 0; cam < 4; cam++) a += pw[cam];
-        a /= 3.0f;
-        const float scale = 1.0f + wv * (a - wv) / (a * a * 3.0f);
-        const float fw = wv / a;
+        a *= (1.0f / 3.0f);
+        const float ra = __frcp_rn(a);
+        const float scale = 1.0f + (wv * (a - wv)) * (ra * ra) * (1.0f / 3.0f);
+        const float fw = wv * ra;
 #pragma unroll
         for (int cam = 0; cam < 4; cam++) pw[cam] *= (cam == worst) ? fw : scale;
     }
@@ -332,6 +333,7 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     __shared__ float *s_cp[4];
     __shared__ float s_pd2r[6], s_chw[3];
     __shared__ float s_tfac[kFac], s_mfac[kFac];
+    __shared__ float s_wnd2[256], s_wi[256]; /* squared window at each pixel, and its reciprocal */
 
     const int tid = threadIdx.x;
     const int l = tid & 7, grp = tid >> 3;
@@ -343,6 +345,12 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     if (tid < 16) {
         const float s = c_hwin[tid];
         s_hsq[tid] = s * s;
+    }
+    __syncthreads();
+    for (int px = tid; px < 256; px += kTexThreads) {
+        const float w2 = s_hsq[sym8(px >> 4)] * s_hsq[sym8(px & 15)];
+        s_wnd2[px] = w2;
+        s_wi[px] = __frcp_rn(w2);
     }
     if (tid < 4) s_cp[tid] = clt[tid];
     if (tid == 0) {
@@ -459,13 +467,13 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
         for (int px = tid; px < 256; px += kTexThreads) {
             const int r = px >> 4, c = px & 15;
             const int e = JT(r, c);
-            const float wnd2 = s_hsq[sym8(r)] * s_hsq[sym8(c)];
+            const float wnd2 = s_wnd2[px], wi = s_wi[px];
             float o[12];
             if (colors == 3)
-                combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, wnd2, p.dust_remove,
+                combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, wnd2, wi, p.dust_remove,
                                  p.keep_weights, o);
             else
-                combine_pixel<1>(s_t, kJob, s_t, kJob, 1.0f, e, s_pd2r, ksigma, s_chw, wnd2, p.dust_remove,
+                combine_pixel<1>(s_t, kJob, s_t, kJob, 1.0f, e, s_pd2r, ksigma, s_chw, wnd2, wi, p.dust_remove,
                                  p.keep_weights, o);
             if (want_tiles) {
                 float *dst = texture_tiles + (size_t)n * texture_stride + px;
