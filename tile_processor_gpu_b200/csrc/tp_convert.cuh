@@ -76,8 +76,9 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
 
     /* (cos, sin)(pi s / 16) for the shifted windows */
     const float xh = shx * (1.0f / 16.0f), xv = shy * (1.0f / 16.0f);
-    const float hc = cospif(xh), hs = sinpif(xh);
-    const float vc = cospif(xv), vs = sinpif(xv);
+    float hc, hs, vc, vs;
+    sincospif(xh, &hs, &hc);
+    sincospif(xv, &vs, &vc);
 
     const int c0 = color & 1, c1 = (color >> 1) & 1;
     const bool fast = (itlx >= 0) && (itlx < g.W - 16) && (itly >= 0) && (itly < g.H - 16);
@@ -169,7 +170,8 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
      * (per row, angles shared across the group) (:2715-2776) ---- */
     {
         const float a = (shx * (float)(2 * l + 1)) * 0.0625f;
-        const float ch = cospif(a), sh = sinpif(a);
+        float ch, sh;
+        sincospif(a, &sh, &ch);
 #pragma unroll
         for (int m = 0; m < 8; m++) {
             const float x0 = cc[m], x1 = sc[m], x2 = cs[m], x3 = ss[m];
@@ -181,7 +183,8 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
     }
     {
         const float a = (shy * (float)(2 * l + 1)) * 0.0625f;
-        const float cvl = cospif(a), svl = sinpif(a);
+        float cvl, svl;
+        sincospif(a, &svl, &cvl);
 #pragma unroll
         for (int m = 0; m < 8; m++) {
             const float cv = __shfl_sync(gm, cvl, m, 8), sv = __shfl_sync(gm, svl, m, 8);
