@@ -33,7 +33,7 @@ __device__ __constant__ int c_rind[16] = TP_RIND_INIT;
  * fetch distinct words in one pass, where the constant cache would serialise
  * them.  Runtime-settable low-pass filters: lpf_data[0..3], lpf_rb_corr,
  * lpf_corr. */
-__device__ float d_lpf[6][64] = TP_LPF_DEFAULT_INIT;
+__device__ __align__(16) float d_lpf[6][64] = TP_LPF_DEFAULT_INIT;
 __device__ float d_alpha_fade[16][256] = TP_ALPHA_FADE_INIT;
 __device__ float d_hwin[16] = TP_HWIN_INIT;
 __device__ float d_hwinc[16] = TP_HWINC_INIT;

@@ -5,13 +5,14 @@
  * corrUnfoldTile :2950-3008).
  *
  * One 8-lane group per (tile, pair) entry of the index list.  Lane l holds
- * column l of the four accumulated quadrants; the color accumulation, the two
- * LPFs and the amplitude normalisation are per coefficient; the vertical
- * DCT-II/DST-II runs on the held column, one shared-memory transpose per
- * quadrant gives rows for the horizontal pass, and the unfold into the
- * (2r+1)^2 output takes the previous row of quadrants 2 and 3 from the lane
- * above by a shuffle.  The output tile is staged in shared memory and written
- * as consecutive floats.
+ * row l of the four accumulated quadrants, loaded as 16-byte vectors; the
+ * color accumulation, the two LPFs and the amplitude normalisation are per
+ * coefficient; the horizontal DCT-II/DST-II runs on the held row, one
+ * shared-memory transpose per quadrant gives columns for the vertical pass
+ * (the separable transform in the other order), and the unfold into the
+ * (2r+1)^2 output reads the pixel-domain quadrants back from shared memory.
+ * The output tile is staged in shared memory and written as consecutive
+ * floats.
  */
 #pragma once
 #include "tp_common.cuh"
@@ -21,6 +22,18 @@ namespace tp {
 /* per-group buffer: four 8x9 quadrants (transpose, then the pixel-domain
  * quadrants), then the (2r+1)^2 output staging; 536 % 32 == 24 */
 constexpr int kCorrBuf = 4 * 72 + 8 + 240;
+
+/* 8 consecutive floats at p (16-byte aligned when al16) */
+__device__ __forceinline__ void load_row8(const float *p, bool al16, float v[8])
+{
+    if (al16) {
+        const float4 x = *reinterpret_cast<const float4 *>(p), y = *reinterpret_cast<const float4 *>(p + 4);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = p[k];
+    }
+}
 
 /* One (tile, pair) correlation on an 8-lane group.  a, b: the two cameras'
  * CLT of the tile, colour c at a + c * cstride (4 x 64 floats, row stride 8);
@@ -32,65 +45,73 @@ __device__ __forceinline__ void corr_job(const float *a, const float *b, int cst
 {
     const int sz = 2 * r + 1;
     float *stage = tb + 296;
-    float acc[4][8];
+    const bool al16 = !((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) |
+                         (uintptr_t)(cstride * sizeof(float))) & 15);
+    float acc[4][8]; /* row l of each quadrant */
 #pragma unroll
     for (int q = 0; q < 4; q++)
 #pragma unroll
-        for (int m = 0; m < 8; m++) acc[q][m] = 0.0f;
+        for (int k = 0; k < 8; k++) acc[q][k] = 0.0f;
     for (int color = 0; color < colors; color++) {
         const float s = color == 0 ? scale0 : color == 1 ? scale1 : scale2;
-        const float *ta = a + color * cstride + l, *tbb = b + color * cstride + l;
+        float A[4][8], B[4][8];
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
-            const int o = m * 8;
-            const float a0 = ta[o], a1 = ta[o + 64], a2 = ta[o + 128], a3 = ta[o + 192];
-            const float b0 = tbb[o], b1 = tbb[o + 64], b2 = tbb[o + 128], b3 = tbb[o + 192];
+        for (int q = 0; q < 4; q++) {
+            load_row8(a + color * cstride + q * 64 + l * 8, al16, A[q]);
+            load_row8(b + color * cstride + q * 64 + l * 8, al16, B[q]);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const float a0 = A[0][k], a1 = A[1][k], a2 = A[2][k], a3 = A[3][k];
+            const float b0 = B[0][k], b1 = B[1][k], b2 = B[2][k], b3 = B[3][k];
             /* CLT-domain correlation of the two tiles */
             const float r0 = __fmaf_rn(a3, b3, __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, a0 * b0)));
             const float r1 = __fmaf_rn(a2, b3, __fmaf_rn(-a3, b2, __fmaf_rn(a0, b1, -a1 * b0)));
             const float r2 = __fmaf_rn(a1, b3, __fmaf_rn(a0, b2, __fmaf_rn(-a3, b1, -a2 * b0)));
             const float r3 = __fmaf_rn(a0, b3, __fmaf_rn(-a1, b2, __fmaf_rn(-a2, b1, a3 * b0)));
-            acc[0][m] = __fmaf_rn(s, r0, acc[0][m]);
-            acc[1][m] = __fmaf_rn(s, r1, acc[1][m]);
-            acc[2][m] = __fmaf_rn(s, r2, acc[2][m]);
-            acc[3][m] = __fmaf_rn(s, r3, acc[3][m]);
+            acc[0][k] = __fmaf_rn(s, r0, acc[0][k]);
+            acc[1][k] = __fmaf_rn(s, r1, acc[1][k]);
+            acc[2][k] = __fmaf_rn(s, r2, acc[2][k]);
+            acc[3][k] = __fmaf_rn(s, r3, acc[3][k]);
         }
         if (color == 1) { /* LPF after red and blue */
+            float f[8];
+            load_row8(&d_lpf[4][l * 8], true, f);
 #pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const float f = __ldg(&d_lpf[4][m * 8 + l]);
+            for (int k = 0; k < 8; k++)
 #pragma unroll
-                for (int q = 0; q < 4; q++) acc[q][m] *= f;
-            }
+                for (int q = 0; q < 4; q++) acc[q][k] *= f[k];
         }
     }
     /* amplitude normalisation with fat zero, then the final LPF */
+    {
+        float f[8];
+        load_row8(&d_lpf[5][l * 8], true, f);
 #pragma unroll
-    for (int m = 0; m < 8; m++) {
-        float s2 = fat_zero * fat_zero;
+        for (int k = 0; k < 8; k++) {
+            float s2 = fat_zero * fat_zero;
 #pragma unroll
-        for (int q = 0; q < 4; q++) s2 = __fmaf_rn(acc[q][m], acc[q][m], s2);
-        const float sc = rsqrtf(s2);
-        const float f = __ldg(&d_lpf[5][m * 8 + l]);
+            for (int q = 0; q < 4; q++) s2 = __fmaf_rn(acc[q][k], acc[q][k], s2);
+            const float sc = rsqrtf(s2);
 #pragma unroll
-        for (int q = 0; q < 4; q++) acc[q][m] = (acc[q][m] * sc) * f;
+            for (int q = 0; q < 4; q++) acc[q][k] = (acc[q][k] * sc) * f[k];
+        }
     }
-    /* pixel domain: vertical DCT-II (q0,q1) / DST-II (q2,q3) on the held
-     * column, transpose, horizontal DCT-II (q0,q2) / DST-II (q1,q3); the
-     * result row l of quadrant q replaces its transpose buffer */
+    /* pixel domain: horizontal DCT-II (q0,q2) / DST-II (q1,q3) on the held
+     * row, transpose, vertical DCT-II (q0,q1) / DST-II (q2,q3) on the held
+     * column, which replaces that column of its transpose buffer */
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        float v[8], row[8];
-        if (q >> 1) dtt8<3>(acc[q], v); else dtt8<2>(acc[q], v);
+        float v[8], col[8];
+        if (q & 1) dtt8<3>(acc[q], v); else dtt8<2>(acc[q], v);
 #pragma unroll
         for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
         __syncwarp(gm);
 #pragma unroll
-        for (int k = 0; k < 8; k++) row[k] = tb[TBI(q, k, l)];
-        __syncwarp(gm);
-        if (q & 1) dtt8<3>(row, v); else dtt8<2>(row, v);
+        for (int k = 0; k < 8; k++) col[k] = tb[TBI(q, k, l)];
+        if (q >> 1) dtt8<3>(col, v); else dtt8<2>(col, v);
 #pragma unroll
-        for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
+        for (int k = 0; k < 8; k++) tb[TBI(q, k, l)] = v[k];
     }
     __syncwarp(gm);
     /* unfold (lane i = rows +-i): R[+-i][+-j] from q0[i][j], q1[i][j-1],
