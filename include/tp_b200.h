@@ -238,6 +238,38 @@ int tp_generate_RBGA(const tp_geometry *g,
                      size_t texture_rbga_stride, float *texture_tiles,
                      tp_stream_t stream);
 
+/* ---- generate_RBGA with library-owned list scratch ------------------------------
+ * No counterpart in the reference: the same work as tp_generate_RBGA, but the
+ * texture list, its eight sub-list counts and the window of interest live in
+ * a fixed device array inside the library instead of caller buffers, so a
+ * caller that cannot allocate device memory (a CUDA graph being captured, a
+ * real-time loop that must not call cudaMalloc, a host binding without a
+ * device allocator) can still run the call.  Limits and rules:
+ *   - scratch: TP_NOALLOC_SCRATCH_INTS ints (1 MiB); frames whose list needs
+ *     more (tilesx * tilesy rounded up to 4 rows, + 16) are rejected with
+ *     TP_ERR_ARG before any device work;
+ *   - the first call on a device looks the array up (cudaGetSymbolAddress);
+ *     make it before capturing a stream into a graph;
+ *   - no state carries from one call to the next (each call rebuilds the
+ *     list); concurrent or overlapping calls on one device share the array
+ *     and race: serialise them (one stream, or events);
+ *   - tasks' bits 0..3 are rewritten with the neighbour mask, as in
+ *     tp_generate_RBGA; the window of interest is not returned. */
+#define TP_NOALLOC_SCRATCH_INTS (1 << 18)
+int tp_generate_RBGA_noalloc(const tp_geometry *g,
+                             tp_task *tasks, int num_tiles,
+                             int width, int height,
+                             float *const *clt,
+                             const float *port_offsets,
+                             int colors, int is_lwir,
+                             float min_shot, float scale_shot,
+                             float diff_sigma, float diff_threshold,
+                             float min_agree,
+                             float weight0, float weight1, float weight2,
+                             int dust_remove, int keep_weights,
+                             size_t texture_rbga_stride, float *texture_tiles,
+                             tp_stream_t stream);
+
 /* ---- the whole hot path for one frame ------------------------------------------
  * No single counterpart in the reference: it runs convert_correct_tiles,
  * correlate2D and generate_RBGA (src/TileProcessor.cuh:1859-1937, :1176-1443,

@@ -102,6 +102,11 @@ def test_rejects_bad_arguments(native):
                                 None)) == N.TP_ERR_ARG
     assert _code(lambda: N.call("tp_disparity_fit", g.ptr, fake, 225, 7, 4, fake, fake, 63, 0, None, fake,
                                 None)) == N.TP_ERR_ARG
+    # no-alloc generate_RBGA: a frame whose list exceeds the library's scratch
+    big = _geom(img_width=8192, img_height=8192)
+    assert _code(lambda: N.call("tp_generate_RBGA_noalloc", big.ptr, fake, 4, 1024, 1024, fake, fake, *args, 0,
+                                8200, fake, None)) == N.TP_ERR_ARG
+    assert "scratch" in N.last_error()
     # LPF table index
     v = np.zeros(64, np.float32)
     assert _code(lambda: N.call("tp_set_lpf", 6, v.ctypes.data_as(P))) == N.TP_ERR_ARG

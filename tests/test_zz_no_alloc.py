@@ -1,0 +1,59 @@
+"""tp_generate_RBGA_noalloc against tp_generate_RBGA: the same overlapped RGBA
+image, on two consecutive calls (the library-owned list scratch carries no
+state from one call to the next).  Collected last, and self-contained, so it
+passes both alone and after the other GPU tests."""
+import numpy as np
+import pytest
+
+from cases import Case, blob_mask
+
+pytestmark = pytest.mark.gpu
+
+TEX = dict(colors=3, is_lwir=0, min_shot=10.0, scale_shot=3.0, diff_sigma=1.5, diff_threshold=10.0, min_agree=3.0,
+           weight0=0.294118, weight1=0.117647, weight2=0.588235, dust_remove=1, keep_weights=0)
+
+
+def _cases():
+    rng = np.random.default_rng(33)
+    sparse = Case(256, 256, seed=9, border_mode=0, mask=blob_mask(rng, 32, 32, 0.3))
+    return {"dense256": Case(256, 256, seed=8, border_mode=0), "sparse256": sparse,
+            "plane512": Case(512, 384, seed=10, border_mode=0, scene="plane")}
+
+
+@pytest.mark.parametrize("name", ["dense256", "sparse256", "plane512"])
+def test_noalloc_matches_generate_rbga(native, name):
+    import torch
+    import gpu_runner as R
+    from tile_processor_gpu_b200 import api
+    c = _cases()[name]
+    fr = R.Frame(c)
+    R.convert(fr)
+    p = TEX
+    args = (p["colors"], p["is_lwir"], p["min_shot"], p["scale_shot"], p["diff_sigma"], p["diff_threshold"],
+            p["min_agree"], p["weight0"], p["weight1"], p["weight2"], p["dust_remove"], p["keep_weights"])
+    stride = (c.TX + 1) * 8 + 40
+    rows = (c.TY + 1) * 8 * 4
+    # the drop-in with caller buffers
+    ref = torch.full((rows + 8, stride), 3.0, device="cuda")
+    tasks = api.tasks_to_device(c.tasks, "cuda")
+    idx = torch.zeros(c.TX * c.TYA + 256, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(8, dtype=torch.int32, device="cuda")
+    woi = torch.zeros(4, dtype=torch.int32, device="cuda")
+    api.generate_RBGA(fr.g, tasks, c.num_tiles, idx, cnt, woi, c.TX, c.TY, fr.p_clt, fr.port_offsets, *args,
+                      stride, ref)
+    torch.cuda.synchronize()
+    want = ref.cpu().numpy()
+    tasks_after = api.tasks_from_device(tasks)
+    # two consecutive no-alloc calls, each on fresh tasks and a dirty output
+    for k in range(2):
+        out = torch.full((rows + 8, stride), 5.0 + k, device="cuda")
+        t2 = api.tasks_to_device(c.tasks, "cuda")
+        api.generate_RBGA_noalloc(fr.g, t2, c.num_tiles, c.TX, c.TY, fr.p_clt, fr.port_offsets, *args, stride, out)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        # the cleared window and everything outside it: identical to the drop-in,
+        # except the untouched area keeps each buffer's own fill
+        touched = want != 3.0
+        assert np.array_equal(got[touched], want[touched]), k
+        assert np.all(got[~touched] == 5.0 + k)
+        assert np.array_equal(api.tasks_from_device(t2)["task"], tasks_after["task"])

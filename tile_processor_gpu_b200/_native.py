@@ -58,6 +58,8 @@ SIGNATURES = {
     "tp_clear_texture_rbga": [_G, _I, _I, _S, _P, _P],
     "tp_generate_RBGA": [_G, _P, _I, _P, _P, _P, _I, _I, _P, _P, _I, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I,
                          _I, _S, _P, _P],
+    "tp_generate_RBGA_noalloc": [_G, _P, _I, _I, _I, _P, _P, _I, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, _I, _S,
+                                 _P, _P],
     "tp_process_frame": [_G, _P, _P, _P, _S, _P, _I, _I, _I, _F, _F, _F, _F, _I, _S, _P, _P, _F, _F, _F, _F, _F,
                          _F, _I, _P, _P, _P, _S, _P, _P, _P],
     "tp_disparity_fit": [_G, _P, _S, _I, _S, _P, _P, _I, _I, _P, _P, _P],

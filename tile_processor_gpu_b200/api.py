@@ -165,6 +165,18 @@ def generate_RBGA(geom, gpu_tasks, num_tiles, gpu_texture_indices, num_texture_t
                  _dptr(gpu_texture_tiles), _stream(stream))
 
 
+def generate_RBGA_noalloc(geom, gpu_tasks, num_tiles, width, height, gpu_clt, gpu_port_offsets, colors, is_lwir,
+                          min_shot, scale_shot, diff_sigma, diff_threshold, min_agree, weight0, weight1, weight2,
+                          dust_remove, keep_weights, texture_rbga_stride, gpu_texture_tiles, stream=None):
+    """generate_RBGA with the texture list in library-owned device scratch
+    (no list buffers from the caller; calls on one device must not overlap)."""
+    _native.call("tp_generate_RBGA_noalloc", geom.ptr, _dptr(gpu_tasks), int(num_tiles), int(width), int(height),
+                 _parr(gpu_clt), _dptr(gpu_port_offsets), int(colors), int(is_lwir), float(min_shot),
+                 float(scale_shot), float(diff_sigma), float(diff_threshold), float(min_agree), float(weight0),
+                 float(weight1), float(weight2), int(dust_remove), int(keep_weights), int(texture_rbga_stride),
+                 _dptr(gpu_texture_tiles), _stream(stream))
+
+
 def process_frame(geom, gpu_kernel_offsets, gpu_kernels, gpu_images, dstride, gpu_tasks, num_tiles, gpu_corrs,
                   corr_stride, gpu_port_offsets, gpu_texture_indices, num_texture_tiles, woi, texture_rbga_stride,
                   gpu_texture_rbga, lpf_mask=0, corr_colors=3, scale0=0.25, scale1=0.25, scale2=0.5, fat_zero=30.0,

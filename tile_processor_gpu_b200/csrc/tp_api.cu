@@ -7,6 +7,7 @@
  * host.
  */
 #include <cuda_runtime.h>
+#include <mutex>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -97,6 +98,31 @@ int texture_smem_setup()
     return cuda_status(cudaFuncSetAttribute(tp::k_textures, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)tp::kTexSmemBytes),
                        "cudaFuncSetAttribute(k_textures)");
+}
+
+/* Scratch of tp_generate_RBGA_noalloc: [0, 8) sub-list counts, [8, 12) window
+ * of interest, [16, ...) the texture list.  Needs no initial contents. */
+static __device__ __align__(256) int g_rbga_scratch[TP_NOALLOC_SCRATCH_INTS];
+
+/* per-device address of g_rbga_scratch, looked up on first use */
+std::mutex g_scratch_mutex;
+int *g_scratch_ptr[128];
+
+int noalloc_scratch(int **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(TP_ERR_NO_DEVICE, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= 128) return fail(TP_ERR_NO_DEVICE, "device %d", dev);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_rbga_scratch);
+        if (e != cudaSuccess) return fail(TP_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+        g_scratch_ptr[dev] = static_cast<int *>(p);
+    }
+    *out = g_scratch_ptr[dev];
+    return TP_OK;
 }
 
 /* host copy of the low-pass tables (last values set by tp_set_lpf) */
@@ -416,6 +442,27 @@ int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *
         tp::k_frame<<<grid, 128, tp::kFrameSmemBytes, s>>>(gd, dstride, kernel_offsets, kernels, images, tasks, num_tiles, parity, fp,
                                          corrs, port_offsets, woi, texture_rbga_stride, texture_rbga, clt);
     return cuda_status(cudaGetLastError(), "process_frame launch");
+}
+
+int tp_generate_RBGA_noalloc(const tp_geometry *g, tp_task *tasks, int num_tiles, int width, int height,
+                             float *const *clt, const float *port_offsets, int colors, int is_lwir, float min_shot,
+                             float scale_shot, float diff_sigma, float diff_threshold, float min_agree,
+                             float weight0, float weight1, float weight2, int dust_remove, int keep_weights,
+                             size_t texture_rbga_stride, float *texture_tiles, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    const long long need = (long long)gd.TX * gd.TYA + 16;
+    if (need > TP_NOALLOC_SCRATCH_INTS)
+        return fail(TP_ERR_ARG, "frame needs %lld scratch ints, the library holds %d (%d x %d tiles max)", need,
+                    TP_NOALLOC_SCRATCH_INTS, gd.TX, (TP_NOALLOC_SCRATCH_INTS - 16) / (gd.TX > 0 ? gd.TX : 1));
+    int *scratch = nullptr;
+    if ((rc = noalloc_scratch(&scratch))) return rc;
+    return tp_generate_RBGA(g, tasks, num_tiles, scratch + 16, scratch, scratch + 8, width, height, clt,
+                            port_offsets, colors, is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold,
+                            min_agree, weight0, weight1, weight2, dust_remove, keep_weights, texture_rbga_stride,
+                            texture_tiles, stream);
 }
 
 int tp_disparity_fit(const tp_geometry *g, const float *corrs, size_t corr_stride, int corr_radius,
