@@ -320,6 +320,34 @@ int tp_disparity_fit(const tp_geometry *g,
                      float *disparity, float *strength,
                      tp_stream_t stream);
 
+/* ---- CLT kernel tables from spatial kernels ------------------------------------
+ * No counterpart in the reference, which reads its tables from files its Java
+ * caller writes (src/dtt8x8.cu:228-238).  psf: device float[n][15][15],
+ * kernel taps -7..7 (rows vertical); clt_kernels: device float[n][4][8][8],
+ * the entry layout of the tables tp_convert_correct_tiles reads (n =
+ * kernels_vert * kernels_hor * 3 for one camera's table).  K_q[u][v] =
+ * sum_mn h[m][n] A(u, m) B(v, n) with A/B = cos or sin(pi tap (2k+1) / 16)
+ * (cosine vertical for CC/SC, horizontal for CC/CS), accumulated in double.
+ * The CLT-domain product approximates the spatial convolution (exact for a
+ * single centre tap; 1.5e-4 relative for a sigma-0.3 px Gaussian, 4% at
+ * 1 px). */
+int tp_psf_to_clt(const float *psf, size_t n, float *clt_kernels, tp_stream_t stream);
+
+/* ---- host helpers for the reference harness's files and lists ------------------
+ * Raw native-endian float32 files without headers (src/dtt8x8.cu:144-165):
+ * returns the number of floats read / written, or TP_ERR_ARG. */
+long long tp_read_floats(const char *path, float *dst, size_t count);
+long long tp_write_floats(const char *path, const float *src, size_t count);
+/* The harness's task list (src/dtt8x8.cu:415-428): one task per tile in
+ * linescan order, bits task_bits, xy[cam] from portsxy[cam] (host
+ * float[tilesy * tilesx][2], the *.portsxy files).  tasks: host array of
+ * tilesx * tilesy.  Returns the number of tasks. */
+int tp_tasks_from_portsxy(const float *const *portsxy, int tilesx, int tilesy, int task_bits, tp_task *tasks);
+/* The harness's correlation list (src/dtt8x8.cu:432-446): (tile << 8) | pair
+ * for every pair bit of every task, in task order (host arrays; NULL
+ * corr_indices only counts).  Returns the number of entries. */
+int tp_corr_indices_from_tasks(const tp_task *tasks, int num_tiles, int tilesx, int *corr_indices);
+
 #ifdef __cplusplus
 }
 #endif

@@ -208,3 +208,21 @@ def fit_profile(S, valid=None, mode=0):
     lib().tpo_fit_profile(_p(S), _p(v), ctypes.c_int((S.size - 1) // 2), ctypes.c_int(mode), ctypes.byref(rho),
                           ctypes.byref(pk))
     return rho.value, pk.value
+
+
+def psf_to_clt(h):
+    """CLT kernel quadrants [..., 4, 8, 8] of spatial kernels h[..., 15, 15]
+    (taps -7..7, rows vertical), FP64, as a direct sum over the taps:
+    K_q[u][v] = sum_mn h[m][n] A(u, m) B(v, n), A = cos (CC, SC) or sin (CS,
+    SS) of pi m (2u+1)/16, B = cos (CC, CS) or sin (SC, SS) of pi n (2v+1)/16."""
+    h = np.asarray(h, dtype=np.float64)
+    taps = np.arange(-7, 8)
+    k = np.arange(8)
+    ang = np.pi * (2 * k[:, None] + 1) * taps[None, :] / 16.0   # [8][15]
+    c, s = np.cos(ang), np.sin(ang)
+    out = np.zeros(h.shape[:-2] + (4, 8, 8))
+    for q, (A, B) in enumerate(((c, c), (c, s), (s, c), (s, s))):
+        for u in range(8):
+            for v in range(8):
+                out[..., q, u, v] = np.sum(h * A[u][:, None] * B[v][None, :], axis=(-2, -1))
+    return out

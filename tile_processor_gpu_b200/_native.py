@@ -63,6 +63,9 @@ SIGNATURES = {
     "tp_process_frame": [_G, _P, _P, _P, _S, _P, _I, _I, _I, _F, _F, _F, _F, _I, _S, _P, _P, _F, _F, _F, _F, _F,
                          _F, _I, _P, _P, _P, _S, _P, _P, _P],
     "tp_disparity_fit": [_G, _P, _S, _I, _S, _P, _P, _I, _I, _P, _P, _P],
+    "tp_psf_to_clt": [_P, _S, _P, _P],
+    "tp_tasks_from_portsxy": [_P, _I, _I, _I, _P],
+    "tp_corr_indices_from_tasks": [_P, _I, _I, _P],
     "tp_set_lpf": [_I, _P],
     "tp_get_lpf": [_I, _P],
     "tp_reset_lpf": [],
@@ -71,6 +74,8 @@ SIGNATURES = {
     "tp_tiles_ya": [_G],
 }
 STRING_FUNCS = ("tp_last_error", "tp_version")
+# entry points returning a count (long long) instead of a status
+COUNT_FUNCS = {"tp_read_floats": [ctypes.c_char_p, _P, _S], "tp_write_floats": [ctypes.c_char_p, _P, _S]}
 
 _lib = None
 
@@ -91,6 +96,10 @@ def load():
         fn = getattr(lib, name)
         fn.argtypes = []
         fn.restype = ctypes.c_char_p
+    for name, argtypes in COUNT_FUNCS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = ctypes.c_longlong
     _lib = lib
     return lib
 

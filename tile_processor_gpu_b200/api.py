@@ -204,6 +204,12 @@ def disparity_fit(geom, gpu_corrs, corr_stride, corr_radius, num_corr_tiles, gpu
                  _dptr(gpu_disparity), _dptr(gpu_strength), _stream(stream))
 
 
+def psf_to_clt(gpu_psf, gpu_clt_kernels, stream=None):
+    """CLT kernel tables [n][4][8][8] from spatial kernels [n][15][15] (device)."""
+    n = gpu_psf.numel() // 225
+    _native.call("tp_psf_to_clt", _dptr(gpu_psf), int(n), _dptr(gpu_clt_kernels), _stream(stream))
+
+
 def set_lpf(which, values):
     """Replace a low-pass table on the current device (0..3 lpf_data, 4 lpf_rb_corr, 5 lpf_corr)."""
     a = np.ascontiguousarray(values, dtype=np.float32).reshape(64)

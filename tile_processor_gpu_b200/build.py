@@ -27,7 +27,8 @@ def nvcc_path():
 
 def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
-                  glob.glob(os.path.join(CSRC, "*.inc")) + glob.glob(os.path.join(_ROOT, "include", "*.h")))
+                  glob.glob(os.path.join(CSRC, "*.cpp")) + glob.glob(os.path.join(CSRC, "*.inc")) +
+                  glob.glob(os.path.join(_ROOT, "include", "*.h")))
 
 
 def needs_build():
@@ -38,10 +39,12 @@ def needs_build():
 
 
 def build(force=False, verbose=False):
-    """Compile csrc/tp_api.cu (which includes every kernel) into libtp_b200.so."""
+    """Compile csrc/tp_api.cu (which includes every kernel) and the host
+    helpers csrc/tp_io.cpp into libtp_b200.so."""
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc_path()] + ARCH_FLAGS + NVCC_FLAGS + ["-o", OUT + ".tmp", os.path.join(CSRC, "tp_api.cu")]
+    cmd = [nvcc_path()] + ARCH_FLAGS + NVCC_FLAGS + ["-o", OUT + ".tmp", os.path.join(CSRC, "tp_api.cu"),
+                                                     os.path.join(CSRC, "tp_io.cpp")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))

@@ -20,6 +20,7 @@
 #include "tp_list.cuh"
 #include "tp_frame.cuh"
 #include "tp_disparity.cuh"
+#include "tp_kernels_gen.cuh"
 
 #define TP_VERSION "tile_processor_gpu_b200 0.1 (sm_100a)"
 
@@ -463,6 +464,18 @@ int tp_generate_RBGA_noalloc(const tp_geometry *g, tp_task *tasks, int num_tiles
                             port_offsets, colors, is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold,
                             min_agree, weight0, weight1, weight2, dust_remove, keep_weights, texture_rbga_stride,
                             texture_tiles, stream);
+}
+
+int tp_psf_to_clt(const float *psf, size_t n, float *clt_kernels, tp_stream_t stream)
+{
+    if (n == 0) return TP_OK;
+    if (!psf || !clt_kernels) return fail(TP_ERR_ARG, "NULL psf / clt_kernels");
+    int sms;
+    int rc = sm_count(&sms);
+    if (rc) return rc;
+    tp::k_psf_to_clt<<<grid_for((long long)n, 1, sms, 8), 256, 0, (cudaStream_t)stream>>>(psf, (long long)n,
+                                                                                         clt_kernels);
+    return cuda_status(cudaGetLastError(), "psf_to_clt launch");
 }
 
 int tp_disparity_fit(const tp_geometry *g, const float *corrs, size_t corr_stride, int corr_radius,
