@@ -12,7 +12,8 @@ HEADER = os.path.join(ROOT, "include", "tp_b200.h")
 
 
 def declared_functions():
-    src = open(HEADER).read()
+    with open(HEADER) as fh:
+        src = fh.read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(tp_\w+)\s*\(", src, flags=re.M)))
 
