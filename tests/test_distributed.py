@@ -38,7 +38,7 @@ def test_two_ranks_gloo():
     import torch.multiprocessing as mp
     port = _free_port()
     world, frames = 2, 9
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port, frames, out), nprocs=world, join=True)
     for rank in range(world):
