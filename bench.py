@@ -54,7 +54,7 @@ FP32_NOMINAL_TFLOPS = 74.4
 # DRAM bytes of each stage of one frame of this workload from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum summed over the stage's
 # launches; profiles/launch_list_2592x1936_quad.md)
-TRAFFIC = {"convert": 1384.7e6, "correlate": 1358.9e6, "texture": 1555.7e6}
+TRAFFIC = {"convert": 1384.2e6, "correlate": 1359.5e6, "texture": 1559.4e6}
 
 
 def peaks():
@@ -341,6 +341,32 @@ def run_b200(args, rank, world, local, pg):
     torch.cuda.synchronize()
     fused_ms = f0.elapsed_time(f1) / fused_steps
 
+    # the same step captured once in a CUDA graph and replayed (17 launches)
+    graph_ms = None
+    try:
+        side = torch.cuda.Stream()
+        side.wait_stream(stream)
+        with torch.cuda.stream(side):
+            pipe.step()
+        stream.wait_stream(side)
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            pipe.step()
+        graph.replay()
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(fused_steps):
+            graph.replay()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        graph_ms = round(g0.elapsed_time(g1) / fused_steps, 4)
+        del graph
+    except Exception as e:  # capture is optional: the eager step is the measurement
+        graph_ms = "capture failed: %s" % str(e).splitlines()[0][:120]
+
     # the disparity fit on the frame's correlations (the consumer of stage 2)
     pipe.step()
     pipe.disparity_fit()
@@ -394,6 +420,7 @@ def run_b200(args, rank, world, local, pg):
                    "l2": "per-step working set %.2f GB > 126 MB L2 (no flush)" % (sum(algo.values()) / 1e9)},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "fused_frame_ms": round(fused_ms, 4),
+        "graph_frame_ms": graph_ms,
         "disparity": disparity,
         "roofline": {"bound": "hbm", "kernel": "k_textures (%s stage)" % dom, "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,

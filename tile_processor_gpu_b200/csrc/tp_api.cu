@@ -93,12 +93,30 @@ unsigned grid_for(long long items, int items_per_block, int sms, int per_sm)
     return (unsigned)need;
 }
 
-/* k_textures takes more than the 48 KB of shared memory granted by default */
+/* Kernels taking more shared memory than the 48 KB granted by default get
+ * their attribute once per device (the first call; make it before capturing
+ * a stream into a graph). */
+std::mutex g_attr_mutex;
+bool g_tex_attr[128], g_frame_attr[128];
+
+int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(TP_ERR_NO_DEVICE, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= 128) return fail(TP_ERR_NO_DEVICE, "device %d", dev);
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    if (done[dev]) return TP_OK;
+    const int rc = cuda_status(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                               what);
+    if (!rc) done[dev] = true;
+    return rc;
+}
+
 int texture_smem_setup()
 {
-    return cuda_status(cudaFuncSetAttribute(tp::k_textures, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)tp::kTexSmemBytes),
-                       "cudaFuncSetAttribute(k_textures)");
+    return set_smem_once(g_tex_attr, (const void *)tp::k_textures, tp::kTexSmemBytes,
+                         "cudaFuncSetAttribute(k_textures)");
 }
 
 /* Scratch of tp_generate_RBGA_noalloc: [0, 8) sub-list counts, [8, 12) window
@@ -434,9 +452,8 @@ int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *
     fp.tex = tex;
     /* odd grid: a grid-stride walk over a raster task list then visits both
      * column parities in every block */
-    if ((rc = cuda_status(cudaFuncSetAttribute(tp::k_frame, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)tp::kFrameSmemBytes),
-                          "cudaFuncSetAttribute(k_frame)")))
+    if ((rc = set_smem_once(g_frame_attr, (const void *)tp::k_frame, tp::kFrameSmemBytes,
+                            "cudaFuncSetAttribute(k_frame)")))
         return rc;
     unsigned grid = grid_for(num_tiles, 4, sms, 3) | 1u;
     for (int parity = 0; parity < 4; parity++)
