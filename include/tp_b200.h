@@ -242,17 +242,21 @@ int tp_generate_RBGA(const tp_geometry *g,
  * No counterpart in the reference: the same work as tp_generate_RBGA, but the
  * texture list, its eight sub-list counts and the window of interest live in
  * a fixed device array inside the library instead of caller buffers, so a
- * caller that cannot allocate device memory (a CUDA graph being captured, a
- * real-time loop that must not call cudaMalloc, a host binding without a
- * device allocator) can still run the call.  Limits and rules:
+ * caller that cannot allocate device memory can still run the call: a
+ * real-time frame loop that must not call cudaMalloc (it synchronises the
+ * whole device and stalls the other streams), or a host binding such as the
+ * reference's Java plugin that reaches the GPU only through buffers it was
+ * handed and has no device allocator of its own.  Limits and rules:
  *   - scratch: TP_NOALLOC_SCRATCH_INTS ints (1 MiB); frames whose list needs
  *     more (tilesx * tilesy rounded up to 4 rows, + 16) are rejected with
  *     TP_ERR_ARG before any device work;
- *   - the first call on a device looks the array up (cudaGetSymbolAddress);
- *     make it before capturing a stream into a graph;
- *   - no state carries from one call to the next (each call rebuilds the
- *     list); concurrent or overlapping calls on one device share the array
- *     and race: serialise them (one stream, or events);
+ *   - the first call on a device, with that device current, looks the
+ *     array up (cudaGetSymbolAddress) once; make that first call before any
+ *     stream capture;
+ *   - every call shares the array and leaves its contents behind; nothing in
+ *     it needs to start at zero (each call clears the part of the list it
+ *     reads and resets the counts and window); calls that overlap on the GPU
+ *     race: serialise them (one stream, or events);
  *   - tasks' bits 0..3 are rewritten with the neighbour mask, as in
  *     tp_generate_RBGA; the window of interest is not returned. */
 #define TP_NOALLOC_SCRATCH_INTS (1 << 18)

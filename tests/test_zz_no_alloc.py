@@ -1,7 +1,13 @@
-"""tp_generate_RBGA_noalloc against tp_generate_RBGA: the same overlapped RGBA
-image, on two consecutive calls (the library-owned list scratch carries no
-state from one call to the next).  Collected last, and self-contained, so it
-passes both alone and after the other GPU tests."""
+"""tp_generate_RBGA_noalloc against tp_generate_RBGA, through the C ABI.
+
+The no-alloc entry point is for callers that cannot allocate device memory --
+a real-time frame loop that must not call cudaMalloc (it synchronises the
+device), or a host binding that only holds the buffers it was handed -- so
+its texture-list scratch is a fixed array inside the library.  The test runs
+it twice in a row and checks both calls give the overlapped RGBA image of the
+entry point with caller buffers: whatever the first call left in the shared
+array must not change the second.  It is collected last and builds its own
+inputs, so it passes both alone and after the other GPU tests."""
 import numpy as np
 import pytest
 

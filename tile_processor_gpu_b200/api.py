@@ -168,8 +168,10 @@ def generate_RBGA(geom, gpu_tasks, num_tiles, gpu_texture_indices, num_texture_t
 def generate_RBGA_noalloc(geom, gpu_tasks, num_tiles, width, height, gpu_clt, gpu_port_offsets, colors, is_lwir,
                           min_shot, scale_shot, diff_sigma, diff_threshold, min_agree, weight0, weight1, weight2,
                           dust_remove, keep_weights, texture_rbga_stride, gpu_texture_tiles, stream=None):
-    """generate_RBGA with the texture list in library-owned device scratch
-    (no list buffers from the caller; calls on one device must not overlap)."""
+    """generate_RBGA with the texture list in library-owned device scratch,
+    for callers that cannot allocate device memory (no list buffers from the
+    caller).  The first call on a device does the set-up; calls that overlap
+    on the GPU race."""
     _native.call("tp_generate_RBGA_noalloc", geom.ptr, _dptr(gpu_tasks), int(num_tiles), int(width), int(height),
                  _parr(gpu_clt), _dptr(gpu_port_offsets), int(colors), int(is_lwir), float(min_shot),
                  float(scale_shot), float(diff_sigma), float(diff_threshold), float(min_agree), float(weight0),
