@@ -121,7 +121,7 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
 {
     __syncwarp(gm);
     const float kshot = rsqrtf(min_shot);
-#pragma unroll 1
+#pragma unroll
     for (int h = 0; h < 2; h++) {
         const int c = l + 8 * h;
         const bool cborder = (c == 0) || (c == 15);
@@ -393,11 +393,16 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
         const int tile = code >> 8;
         return ((code & (1 << 7)) && tile >= 0 && tile < ntiles) ? tile : -1;
     };
-    /* RGBA address of pixel px (slice 0) under `tile`, or NULL when it lies
-     * left of / above the window */
-    auto rgba_at = [&](int tile, int px) -> float * {
+    /* window position of a tile's top-left pixel (once per tile) */
+    auto rgba_origin = [&](int tile, int *gy0, int *gx0) {
         const int ty = tile / g.TX, tx = tile - ty * g.TX;
-        const long long gy = (long long)(ty - wy0) * 8 + (px >> 4), gx = (long long)(tx - wx0) * 8 + (px & 15);
+        *gy0 = (ty - wy0) * 8;
+        *gx0 = (tx - wx0) * 8;
+    };
+    /* RGBA address of pixel px (slice 0) of the tile at (gy0, gx0), or NULL
+     * when it lies left of / above the window */
+    auto rgba_at = [&](int gy0, int gx0, int px) -> float * {
+        const int gy = gy0 + (px >> 4), gx = gx0 + (px & 15);
         if (gy < 0 || gx < 0) return nullptr;
         return texture_rbg + (size_t)gy * texture_rbg_stride + (size_t)gx;
     };
@@ -409,9 +414,11 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
         const int code = lst[n];
         const int tile = code >> 8;
         if (!(code & (1 << 7)) || tile < 0 || tile >= ntiles || !(code & TP_TASK_TEXTURE_BITS)) return;
+        int gy0, gx0;
+        rgba_origin(tile, &gy0, &gx0);
 #pragma unroll
         for (int px = tid; px < 256; px += kTexThreads) {
-            const float *b = rgba_at(tile, px);
+            const float *b = rgba_at(gy0, gx0, px);
             if (!b) continue;
             for (int sl = 0; sl <= colors; sl++) cp_async4(s_r + sl * 256 + px, b + (size_t)sl * slice_stride);
         }
@@ -467,6 +474,8 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
         /* ---- stages 3-4: fuse the four cameras at the thread's pixels and
          * write them out ---- */
         const int nbr = code & TP_TASK_TEXTURE_BITS;
+        int gy0 = 0, gx0 = 0;
+        if (want_rbg && nbr) rgba_origin(tile, &gy0, &gx0);
 #pragma unroll 1
         for (int px = tid; px < 256; px += kTexThreads) {
             const int r = px >> 4, c = px & 15;
@@ -486,7 +495,7 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
                     if (sl < ns_tiles) dst[sl * 256] = o[sl];
             }
             if (want_rbg && nbr) {
-                float *b = rgba_at(tile, px);
+                float *b = rgba_at(gy0, gx0, px);
                 if (b) {
                     const float f = (nbr != TP_TASK_TEXTURE_BITS) ? __ldg(&d_alpha_fade[nbr][px]) : 1.0f;
 #pragma unroll
