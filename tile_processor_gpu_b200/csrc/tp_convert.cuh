@@ -51,7 +51,7 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
                                             const float *__restrict__ kern_tab,
                                             const float *__restrict__ img, float cx, float cy,
                                             int color, int lpf_mask, float *__restrict__ out,
-                                            float (*tb)[9], int l, unsigned gm)
+                                            float (*tb)[9], int l, unsigned gm, const float *pre_ex = nullptr)
 {
     /* ---- kernel tile, integer corner, residual shift (float32, as the
      * reference computes them: src/TileProcessor.cuh:3129-3255) ---- */
@@ -63,10 +63,11 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
     const float kdx = (cx - (float)(ktx << g.ls)) + (float)(1 << (g.ls - 1));
     const float kdy = (cy - (float)(kty << g.ls)) + (float)(1 << (g.ls - 1));
     const size_t kidx = ((size_t)ktx + (size_t)kty * g.KH) * 3 + color;
+    /* the kernel tile's offsets: prefetched by the caller (pre_ex[6]) or here */
     const float *ex = extra_tab + kidx * 8;
-    const float data_x = __ldg(ex + 0), data_y = __ldg(ex + 1);
-    const float dxc_dx = __ldg(ex + 4), dxc_dy = __ldg(ex + 5);
-    const float dyc_dx = __ldg(ex + 6), dyc_dy = __ldg(ex + 7);
+    const float data_x = pre_ex ? pre_ex[0] : __ldg(ex + 0), data_y = pre_ex ? pre_ex[1] : __ldg(ex + 1);
+    const float dxc_dx = pre_ex ? pre_ex[2] : __ldg(ex + 4), dxc_dy = pre_ex ? pre_ex[3] : __ldg(ex + 5);
+    const float dyc_dx = pre_ex ? pre_ex[4] : __ldg(ex + 6), dyc_dy = pre_ex ? pre_ex[5] : __ldg(ex + 7);
     const float px = (cx - 8.0f) - __fmaf_rn(dxc_dy, kdy, __fmaf_rn(dxc_dx, kdx, data_x));
     const float py = (cy - 8.0f) - __fmaf_rn(dyc_dy, kdy, __fmaf_rn(dyc_dx, kdx, data_y));
     const int itlx = corner_clamp(__float2int_rd(px + 0.5f), g.W, true, g.border_mode);
@@ -224,21 +225,52 @@ __global__ void __launch_bounds__(256, 2) k_convert_correct_tiles(
     const unsigned gm = group_mask();
     const int warps_total = gridDim.x * (blockDim.x >> 5);
     const int chunks = (num_tiles + 3) >> 2;
-    for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < chunks * 12; w += warps_total) {
+    /* the task fields of this group's job, read one job ahead so that the
+     * load overlaps the previous job */
+    auto fetch = [&](int w, int *task, int *txy, float *cx, float *cy) {
+        *task = 0;
+        if (w >= chunks * 12) return;
+        const int chunk = w / 12, r = w - chunk * 12, cam = r & 3;
+        const int n = chunk * 4 + ((threadIdx.x >> 3) & 3);
+        if (n >= num_tiles) return;
+        const tp_task *t = tasks + n;
+        *task = __ldg(&t->task);
+        *txy = __ldg(&t->txy);
+        *cx = __ldg(&t->xy[cam][0]);
+        *cy = __ldg(&t->xy[cam][1]);
+    };
+    /* its kernel tile's offsets (the kernel-tile choice of convert_job) */
+    auto fetch_extra = [&](int w, float cx, float cy, float ex[6]) {
+        const int r = w % 12, color = r >> 2, cam = r & 3;
+        const float step_inv = __int_as_float((127 - g.ls) << 23);
+        const int ktx = min(g.KH - 1, max(0, __float2int_rn(__fmaf_rn(cx, step_inv, 1.0f))));
+        const int kty = min(g.KV - 1, max(0, __float2int_rn(__fmaf_rn(cy, step_inv, 1.0f))));
+        const float *e = kernel_offsets[cam] + (((size_t)ktx + (size_t)kty * g.KH) * 3 + color) * 8;
+        ex[0] = __ldg(e + 0); ex[1] = __ldg(e + 1);
+        ex[2] = __ldg(e + 4); ex[3] = __ldg(e + 5);
+        ex[4] = __ldg(e + 6); ex[5] = __ldg(e + 7);
+    };
+    int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int ntask = 0, ntxy = 0;
+    float ncx = 0.0f, ncy = 0.0f, nex[6];
+    fetch(w, &ntask, &ntxy, &ncx, &ncy);
+    if (ntask) fetch_extra(w, ncx, ncy, nex);
+    for (; w < chunks * 12; w += warps_total) {
         const int chunk = w / 12, r = w - chunk * 12;
         const int color = r >> 2, cam = r & 3;
-        const int n = chunk * 4 + ((threadIdx.x >> 3) & 3);
-        if (n >= num_tiles) continue;
-        const tp_task *t = tasks + n;
-        const int task = t->task;
+        const int task = ntask, txy = ntxy;
+        const float cx = ncx, cy = ncy;
+        float ex[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) ex[i] = nex[i];
+        fetch(w + warps_total, &ntask, &ntxy, &ncx, &ncy);
+        if (ntask) fetch_extra(w + warps_total, ncx, ncy, nex);
         if (!task) continue;
-        const int txy = t->txy;
         const int tx = txy & 0xfff, ty = txy >> 16;
         if (tx >= g.TX || ty < 0 || ty >= g.TY) continue;
-        const float cx = t->xy[cam][0], cy = t->xy[cam][1];
         float *out = clt[cam] + (((size_t)ty * g.TX + tx) * 3 + color) * 256;
         convert_job(g, dstride, kernel_offsets[cam], kernels[cam], images[cam], cx, cy, color,
-                    lpf_mask, out, tbuf[grp], l, gm);
+                    lpf_mask, out, tbuf[grp], l, gm, ex);
     }
 }
 
