@@ -219,21 +219,41 @@ class FramePipeline:
             n += np.unique(kx + ky * gd["kernels_hor"]).size * 3
         return n
 
-    # stage calls (each is a C ABI call on the current stream)
-    def convert(self):
-        self.api.convert_correct_tiles(self.g, self.p_extra, self.p_kernels, self.p_images, self.tasks, self.p_clt,
+    # stage calls (each is a C ABI call on the current stream); `slot` selects
+    # another frame's images and outputs (see add_slot), None the main ones
+    def convert(self, slot=None):
+        p_images = self.p_images if slot is None else slot["p_images"]
+        self.api.convert_correct_tiles(self.g, self.p_extra, self.p_kernels, p_images, self.tasks, self.p_clt,
                                        self.dstride, self.num_tiles, 0)
 
-    def correlate(self):
+    def correlate(self, slot=None):
+        corrs = self.corrs if slot is None else slot["corrs"]
         self.api.correlate2D(self.g, self.p_clt, 3, 0.25, 0.25, 0.5, FAT_ZERO, self.num_corr, self.corr_idx,
-                             self.corr_stride, CORR_RADIUS, self.corrs)
+                             self.corr_stride, CORR_RADIUS, corrs)
 
-    def texture(self):
+    def texture(self, slot=None):
         t = TEXTURE
+        rgba = self.rgba if slot is None else slot["rgba"]
         self.api.generate_RBGA(self.g, self.tasks, self.num_tiles, self.tex_indices, self.num_tex, self.woi, self.TX,
                                self.TY, self.p_clt, self.port_offsets, t["colors"], t["is_lwir"], t["min_shot"],
                                t["scale_shot"], t["diff_sigma"], t["diff_threshold"], t["min_agree"], t["weight0"],
-                               t["weight1"], t["weight2"], t["dust_remove"], 0, self.rgba_stride, self.rgba)
+                               t["weight1"], t["weight2"], t["dust_remove"], 0, self.rgba_stride, rgba)
+
+    def add_slot(self, device):
+        """Device images and outputs plus pinned host outputs of one more
+        frame in flight (the CLT, tasks and lists are used within one frame's
+        compute and stay shared)."""
+        torch = self.torch
+        images = [torch.empty_like(x) for x in self.images]
+        return {"images": images, "p_images": self.api.PointerArray(images),
+                "corrs": torch.empty_like(self.corrs), "rgba": torch.empty_like(self.rgba),
+                "host_corrs": torch.empty_like(self.corrs, device="cpu").pin_memory(),
+                "host_rgba": torch.empty_like(self.rgba, device="cpu").pin_memory()}
+
+    def step_slot(self, slot):
+        self.convert(slot)
+        self.correlate(slot)
+        self.texture(slot)
 
     def frame(self):
         t = TEXTURE
@@ -383,21 +403,49 @@ def run_b200(args, rank, world, local, pg):
     disparity["fit_ms"] = round(fit_ms, 4)
 
     # ---- end to end through the public API with host buffers ----
-    e2e_steps = max(2, min(args.steps, 10))
+    # Every frame: its four images from pinned host memory to the device, the
+    # three calls, its correlation tiles and RGBA image back to pinned host
+    # memory.  Two frames in flight on three streams (copy in, compute, copy
+    # out), so the PCIe transfers of one frame overlap the compute of another;
+    # a frame's upload waits for the compute of the frame two before it (same
+    # slot), its compute for its upload and for that frame's download.
+    e2e_steps = max(4, min(args.steps, 30))
     h2d = sum(h.numel() * 4 for h in pipe.host_images)
     d2h = pipe.corrs.numel() * 4 + pipe.rgba.numel() * 4
+    slots = [pipe.add_slot(dev), pipe.add_slot(dev)]
+    s_in, s_comp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    ev = lambda: torch.cuda.Event(enable_timing=False)
+    in_done, comp_done, out_done = [ev(), ev()], [ev(), ev()], [ev(), ev()]
     barrier(pg)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        for c in range(4):
-            pipe.images[c].copy_(pipe.host_images[c], non_blocking=True)
-        pipe.step()
-        pipe.host_corrs.copy_(pipe.corrs, non_blocking=True)
-        pipe.host_rgba.copy_(pipe.rgba, non_blocking=True)
-    e1.record(stream)
+    e0.record(s_in)
+    s_comp.wait_stream(s_in)
+    s_out.wait_stream(s_in)
+    for i in range(e2e_steps):
+        k = i & 1
+        sl = slots[k]
+        with torch.cuda.stream(s_in):
+            if i >= 2:
+                s_in.wait_event(comp_done[k])
+            for c in range(4):
+                sl["images"][c].copy_(pipe.host_images[c], non_blocking=True)
+            in_done[k].record(s_in)
+        with torch.cuda.stream(s_comp):
+            s_comp.wait_event(in_done[k])
+            if i >= 2:
+                s_comp.wait_event(out_done[k])
+            pipe.step_slot(sl)
+            comp_done[k].record(s_comp)
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(comp_done[k])
+            sl["host_corrs"].copy_(sl["corrs"], non_blocking=True)
+            sl["host_rgba"].copy_(sl["rgba"], non_blocking=True)
+            out_done[k].record(s_out)
+    s_out.wait_stream(s_comp)
+    s_out.wait_stream(s_in)
+    e1.record(s_out)
     torch.cuda.synchronize()
     barrier(pg)
     e2e_ms = max_over_ranks(pg, e0.elapsed_time(e1)) / e2e_steps
@@ -428,7 +476,8 @@ def run_b200(args, rank, world, local, pg):
                      "fp32_simt": {"flops": int(flops), "achieved_tflops": round(flops / (stage_ms[dom] * 1e-3) / 1e12, 2),
                                    "nominal_peak_tflops": FP32_NOMINAL_TFLOPS}},
         "e2e": {"value": round(world / (e2e_ms * 1e-3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h), "frames": e2e_steps,
+                "overlap": "two frames in flight: copy-in, compute, copy-out streams"},
         "gpu_launches": int(args.steps * sum(pipe.LAUNCHES.values())),
         "clocks": clocks,
     }
