@@ -352,6 +352,40 @@ int tp_tasks_from_portsxy(const float *const *portsxy, int tilesx, int tilesy, i
  * corr_indices only counts).  Returns the number of entries. */
 int tp_corr_indices_from_tasks(const tp_task *tasks, int num_tiles, int tilesx, int *corr_indices);
 
+/* ---- learned disparity residual -------------------------------------------------
+ * No counterpart in the reference (its Java caller, absent, fits disparity).
+ * A small MLP refines tp_disparity_fit: features = a tile's six (2r+1)^2
+ * correlation planes scaled by their largest magnitude; network 6(2r+1)^2 ->
+ * 256 -> 128 -> 2 with GELU; outputs a correction to the plain fit and a
+ * log-variance.  These are its building blocks (device pointers, row-major
+ * float32, rows = samples); tile_processor_gpu_b200.disparity_net drives
+ * them for inference and training. */
+/* features[tile][p * (2r+1)^2 + k]: the tile's run of correlation entries
+ * (adjacent in corr_indices), pair p in slot p, unlisted pairs zero; rows of
+ * tiles without entries are not written.  feature_stride >= 6 (2r+1)^2. */
+int tp_mlp_features(const tp_geometry *g, const float *corrs, size_t corr_stride, int corr_radius,
+                    size_t num_corr_tiles, const int *corr_indices, float *features, size_t feature_stride,
+                    tp_stream_t stream);
+/* C = beta C + op(A) op(B) (+ bias), op(A) M x K (A[m][k], or A[k][m] when
+ * trans_a), op(B) K x N; with z non-NULL, z = that pre-activation and
+ * C = gelu(z) (exact, erf form). */
+int tp_mlp_gemm(int M, int N, int K, const float *A, int lda, int trans_a, const float *B, int ldb, int trans_b,
+                float beta, float *C, int ldc, const float *bias, float *z, int ldz, tp_stream_t stream);
+/* dz = dh * gelu'(z), rows x cols, leading dimension ld */
+int tp_mlp_gelu_backward(int rows, int cols, int ld, const float *z, const float *dh, float *dz,
+                         tp_stream_t stream);
+/* out[c] = scale * sum over rows of x[r][c] */
+int tp_mlp_colsum(int rows, int cols, int ld, const float *x, float scale, float *out, tp_stream_t stream);
+/* Gaussian negative log-likelihood of out[r] = {d, s} against target[r]:
+ * loss_rows[r] = w[r] (0.5 exp(-s) (d - target)^2 + 0.5 s), s clamped to
+ * [-12, 12]; dout = the gradient of inv_count * sum loss_rows.  w may be NULL
+ * (all ones). */
+int tp_mlp_nll(int rows, const float *out, const float *target, const float *w, float inv_count, float *dout,
+               float *loss_rows, tp_stream_t stream);
+/* Adam step `step` (1, 2, ...) on n parameters */
+int tp_mlp_adam(size_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1, float beta2,
+                float eps, int step, tp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

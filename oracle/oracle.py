@@ -226,3 +226,49 @@ def psf_to_clt(h):
             for v in range(8):
                 out[..., q, u, v] = np.sum(h * A[u][:, None] * B[v][None, :], axis=(-2, -1))
     return out
+
+
+# ---- the learned disparity residual (FP64 restatement of the tp_mlp_* math) --
+def mlp_gelu(x):
+    from scipy.special import erf
+    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+
+
+def mlp_gelu_grad(x):
+    from scipy.special import erf
+    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+
+
+def mlp_forward(p, x):
+    """x [n][1350] -> (out [n][2], cache)"""
+    P = {k: np.asarray(v, np.float64) for k, v in p.items()}
+    z1 = x @ P["W1"] + P["b1"]
+    h1 = mlp_gelu(z1)
+    z2 = h1 @ P["W2"] + P["b2"]
+    h2 = mlp_gelu(z2)
+    out = h2 @ P["W3"] + P["b3"]
+    return out, (x, z1, h1, z2, h2)
+
+
+def mlp_loss_and_grads(p, x, target, w=None):
+    """mean over rows with weight 1 of 0.5 exp(-s) (d - target)^2 + 0.5 s
+    (s clamped to [-12, 12]) and its gradients w.r.t. every parameter"""
+    P = {k: np.asarray(v, np.float64) for k, v in p.items()}
+    x = np.asarray(x, np.float64)
+    out, (_, z1, h1, z2, h2) = mlp_forward(P, x)
+    w = np.ones(len(x)) if w is None else np.asarray(w, np.float64)
+    cnt = max(w.sum(), 1.0)
+    d, s_raw = out[:, 0], out[:, 1]
+    s = np.clip(s_raw, -12.0, 12.0)
+    e = d - target
+    iv = np.exp(-s)
+    loss = (w * (0.5 * iv * e * e + 0.5 * s)).sum() / cnt
+    dout = np.zeros_like(out)
+    dout[:, 0] = w * iv * e / cnt
+    dout[:, 1] = np.where((s_raw > -12.0) & (s_raw < 12.0), w * (0.5 - 0.5 * iv * e * e) / cnt, 0.0)
+    g = {"W3": h2.T @ dout, "b3": dout.sum(0)}
+    dz2 = (dout @ P["W3"].T) * mlp_gelu_grad(z2)
+    g["W2"], g["b2"] = h1.T @ dz2, dz2.sum(0)
+    dz1 = (dz2 @ P["W2"].T) * mlp_gelu_grad(z1)
+    g["W1"], g["b1"] = x.T @ dz1, dz1.sum(0)
+    return loss, g

@@ -7,6 +7,7 @@
  * host.
  */
 #include <cuda_runtime.h>
+#include <math.h>
 #include <mutex>
 #include <stdarg.h>
 #include <stdio.h>
@@ -21,6 +22,7 @@
 #include "tp_frame.cuh"
 #include "tp_disparity.cuh"
 #include "tp_kernels_gen.cuh"
+#include "tp_mlp.cuh"
 
 #define TP_VERSION "tile_processor_gpu_b200 0.1 (sm_100a)"
 
@@ -481,6 +483,89 @@ int tp_generate_RBGA_noalloc(const tp_geometry *g, tp_task *tasks, int num_tiles
                             port_offsets, colors, is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold,
                             min_agree, weight0, weight1, weight2, dust_remove, keep_weights, texture_rbga_stride,
                             texture_tiles, stream);
+}
+
+int tp_mlp_features(const tp_geometry *g, const float *corrs, size_t corr_stride, int corr_radius,
+                    size_t num_corr_tiles, const int *corr_indices, float *features, size_t feature_stride,
+                    tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (corr_radius < 0 || corr_radius > TP_MAX_CORR_RADIUS)
+        return fail(TP_ERR_ARG, "corr_radius %d outside 0..%d", corr_radius, TP_MAX_CORR_RADIUS);
+    const int n2 = (2 * corr_radius + 1) * (2 * corr_radius + 1);
+    if (num_corr_tiles == 0) return TP_OK;
+    if (!corrs || !corr_indices || !features) return fail(TP_ERR_ARG, "NULL corrs / corr_indices / features");
+    if (corr_stride < (size_t)n2) return fail(TP_ERR_ARG, "corr_stride %zu < %d", corr_stride, n2);
+    if (feature_stride < (size_t)(6 * n2)) return fail(TP_ERR_ARG, "feature_stride %zu < %d", feature_stride, 6 * n2);
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    tp::k_mlp_features<<<grid_for((long long)num_corr_tiles, 8, sms, 8), 256, 0, (cudaStream_t)stream>>>(
+        gd.TX * gd.TY, corrs, corr_stride, n2, (long long)num_corr_tiles, corr_indices, features, feature_stride);
+    return cuda_status(cudaGetLastError(), "mlp_features launch");
+}
+
+int tp_mlp_gemm(int M, int N, int K, const float *A, int lda, int trans_a, const float *B, int ldb, int trans_b,
+                float beta, float *C, int ldc, const float *bias, float *z, int ldz, tp_stream_t stream)
+{
+    if (M < 0 || N < 0 || K < 0) return fail(TP_ERR_ARG, "gemm %d x %d x %d", M, N, K);
+    if (M == 0 || N == 0) return TP_OK;
+    if (!A || !B || !C) return fail(TP_ERR_ARG, "NULL gemm operand");
+    if (lda < (trans_a ? M : K) || ldb < (trans_b ? K : N) || ldc < N || (z && ldz < N))
+        return fail(TP_ERR_ARG, "gemm leading dimension too small");
+    if ((M + tp::kGB - 1) / tp::kGB > 65535) return fail(TP_ERR_ARG, "gemm M %d too large", M);
+    dim3 grid((unsigned)((N + tp::kGB - 1) / tp::kGB), (unsigned)((M + tp::kGB - 1) / tp::kGB), 1);
+    tp::k_gemm<<<grid, 256, 0, (cudaStream_t)stream>>>(M, N, K, A, lda, trans_a, B, ldb, trans_b, beta, C, ldc, bias,
+                                                       z, ldz);
+    return cuda_status(cudaGetLastError(), "mlp_gemm launch");
+}
+
+int tp_mlp_gelu_backward(int rows, int cols, int ld, const float *z, const float *dh, float *dz, tp_stream_t stream)
+{
+    if (rows < 0 || cols < 0 || ld < cols) return fail(TP_ERR_ARG, "gelu_backward %d x %d ld %d", rows, cols, ld);
+    if (!rows || !cols) return TP_OK;
+    if (!z || !dh || !dz) return fail(TP_ERR_ARG, "NULL gelu_backward operand");
+    int sms, rc;
+    if ((rc = sm_count(&sms))) return rc;
+    const long long n = (long long)rows * cols;
+    tp::k_gelu_backward<<<grid_for(n, 256, sms, 8), 256, 0, (cudaStream_t)stream>>>(n, cols, ld, z, dh, dz);
+    return cuda_status(cudaGetLastError(), "mlp_gelu_backward launch");
+}
+
+int tp_mlp_colsum(int rows, int cols, int ld, const float *x, float scale, float *out, tp_stream_t stream)
+{
+    if (rows < 0 || cols < 0 || ld < cols) return fail(TP_ERR_ARG, "colsum %d x %d ld %d", rows, cols, ld);
+    if (!cols) return TP_OK;
+    if ((rows && !x) || !out) return fail(TP_ERR_ARG, "NULL colsum operand");
+    tp::k_colsum<<<(cols + 127) / 128, 128, 0, (cudaStream_t)stream>>>(rows, cols, ld, x, scale, out);
+    return cuda_status(cudaGetLastError(), "mlp_colsum launch");
+}
+
+int tp_mlp_nll(int rows, const float *out, const float *target, const float *w, float inv_count, float *dout,
+               float *loss_rows, tp_stream_t stream)
+{
+    if (rows < 0) return fail(TP_ERR_ARG, "nll rows %d", rows);
+    if (!rows) return TP_OK;
+    if (!out || !target || !dout || !loss_rows) return fail(TP_ERR_ARG, "NULL nll operand");
+    tp::k_nll<<<(rows + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rows, out, target, w, inv_count, dout,
+                                                                    loss_rows);
+    return cuda_status(cudaGetLastError(), "mlp_nll launch");
+}
+
+int tp_mlp_adam(size_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1, float beta2,
+                float eps, int step, tp_stream_t stream)
+{
+    if (step < 1) return fail(TP_ERR_ARG, "adam step %d < 1", step);
+    if (!n) return TP_OK;
+    if (!param || !grad || !m || !v) return fail(TP_ERR_ARG, "NULL adam operand");
+    int sms, rc;
+    if ((rc = sm_count(&sms))) return rc;
+    const float c1 = (float)(1.0 / (1.0 - pow((double)beta1, step)));
+    const float c2 = (float)(1.0 / (1.0 - pow((double)beta2, step)));
+    tp::k_adam<<<grid_for((long long)n, 256, sms, 8), 256, 0, (cudaStream_t)stream>>>((long long)n, param, grad, m, v,
+                                                                                   lr, beta1, beta2, eps, c1, c2);
+    return cuda_status(cudaGetLastError(), "mlp_adam launch");
 }
 
 int tp_psf_to_clt(const float *psf, size_t n, float *clt_kernels, tp_stream_t stream)

@@ -201,9 +201,15 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
         o[COLORS + 5 + COLORS] = sqrtf(sw);
     }
     /* wi = 1 / wnd2 correctly rounded (the reference forms it in double).
-     * The weights use the hardware exponential: its relative error (below
-     * 1e-6 wherever a weight is above the 1e-4 floor) is under what float32
-     * inputs already move them by. */
+     * A weight is exp(...) plus the 1e-4 floor added in double and rounded
+     * once to float, as the reference's double floor constant makes it: the
+     * floor sum decides the best and worst cameras where every exponential
+     * is tiny (high-contrast or high-dynamic-range tiles), and a float sum
+     * with 1e-4f can land one ulp lower and break such ties the other way
+     * (splitting the floor into two floats still rounds 1 in 2e6 tiny sums
+     * differently).  The exponential itself is the hardware one: its
+     * relative error (below 1e-6 wherever a weight is above the floor) is
+     * under what float32 inputs already move it by. */
     float pw[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     {
         int k = 0;
@@ -217,7 +223,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
                     const float dc = (D[i][col] - D[j][col]) * wi;
                     d = __fmaf_rn(chw[col] * dc, dc, d);
                 }
-                const float x = __expf(-pd2r[k] * d) + 1e-4f;
+                const float x = __double2float_rn((double)__expf(-pd2r[k] * d) + 1e-4);
                 pw[i] += x;
                 pw[j] += x;
                 k++;
@@ -256,7 +262,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
             const float dc = (D[cam][col] - avg[col]) * wi;
             d2 = __fmaf_rn(chw[col] * dc, dc, d2);
         }
-        pw[cam] = __expf(-ksigma * d2) + 1e-4f;
+        pw[cam] = __double2float_rn((double)__expf(-ksigma * d2) + 1e-4);
     }
     if (dust_remove) {
         int worst = 0;
