@@ -382,6 +382,15 @@ int tp_mlp_colsum(int rows, int cols, int ld, const float *x, float scale, float
  * (all ones). */
 int tp_mlp_nll(int rows, const float *out, const float *target, const float *w, float inv_count, float *dout,
                float *loss_rows, tp_stream_t stream);
+/* Inference on the tensor cores: the weights packed once per update
+ * (w1t: device uint16 [256][1408], W1^T in BF16, zero padded; w2t: device
+ * uint16 [128][256], W2^T in BF16), then out[r] = {d, s} for feature rows x
+ * (rows x 1350, leading dimension ldx), layers 1 and 2 as BF16 tcgen05 MMAs
+ * with FP32 accumulation.  err (device int, may be NULL) is set to 1 if a
+ * wait for the tensor cores ran out (no result then). */
+int tp_mlp_pack(const float *W1, const float *W2, void *w1t, void *w2t, tp_stream_t stream);
+int tp_mlp_infer_tc(int rows, const float *x, int ldx, const void *w1t, const float *b1, const void *w2t,
+                    const float *b2, const float *W3, const float *b3, float *out, int *err, tp_stream_t stream);
 /* Adam step `step` (1, 2, ...) on n parameters */
 int tp_mlp_adam(size_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1, float beta2,
                 float eps, int step, tp_stream_t stream);

@@ -130,3 +130,31 @@ def test_learned_residual_beats_plain_fit(native):
     print("\nheld-out: plain %s  learned %s  mean |err| low/high variance %.4f / %.4f" % (a_plain, a_net, lo, hi))
     assert a_net["rmse_px"] < a_plain["rmse_px"]
     assert hi > lo
+
+
+@pytest.mark.parametrize("rows", [200, 5000])
+def test_tensor_core_inference_matches_fp32(native, rows):
+    """tp_mlp_infer_tc (BF16 tcgen05 MMAs, FP32 accumulation) against the
+    FP32 forward pass: outputs within the BF16 rounding of the operands."""
+    import torch
+    from tile_processor_gpu_b200 import disparity_net as D
+    rng = np.random.default_rng(rows)
+    p = D.init_params(7)
+    for k in p:
+        if k.startswith("b"):
+            p[k] = rng.normal(0, 0.1, p[k].shape).astype(np.float32)
+    x = rng.uniform(-1, 1, (rows, D.N_IN)).astype(np.float32)
+    net = D.DisparityMLP(p)
+    xd = _dev(x)
+    ref = net.forward(xd, rows).clone()
+    net.pack()
+    out = torch.full((rows, 2), -99.0, device="cuda")
+    net.infer_tc(xd, rows, out)
+    torch.cuda.synchronize()
+    assert int(net.tc_err.item()) == 0
+    r, o = ref.cpu().numpy(), out.cpu().numpy()
+    scale = np.abs(r).max(axis=0)
+    err = np.abs(o - r).max(axis=0) / scale
+    print("\ntensor-core vs fp32, rows %d: max rel err %s" % (rows, err))
+    assert np.all(err < 3e-2)
+    assert np.sqrt(np.mean((o - r) ** 2)) / np.sqrt(np.mean(r ** 2)) < 1e-2

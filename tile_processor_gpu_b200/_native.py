@@ -71,6 +71,8 @@ SIGNATURES = {
     "tp_mlp_gelu_backward": [_I, _I, _I, _P, _P, _P, _P],
     "tp_mlp_colsum": [_I, _I, _I, _P, _F, _P, _P],
     "tp_mlp_nll": [_I, _P, _P, _P, _F, _P, _P, _P],
+    "tp_mlp_pack": [_P, _P, _P, _P, _P],
+    "tp_mlp_infer_tc": [_I, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "tp_mlp_adam": [_S, _P, _P, _P, _P, _F, _F, _F, _F, _I, _P],
     "tp_set_lpf": [_I, _P],
     "tp_get_lpf": [_I, _P],

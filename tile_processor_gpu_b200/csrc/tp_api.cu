@@ -99,7 +99,7 @@ unsigned grid_for(long long items, int items_per_block, int sms, int per_sm)
  * their attribute once per device (the first call; make it before capturing
  * a stream into a graph). */
 std::mutex g_attr_mutex;
-bool g_tex_attr[128], g_frame_attr[128];
+bool g_tex_attr[128], g_frame_attr[128], g_tc_attr[128];
 
 int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
 {
@@ -551,6 +551,37 @@ int tp_mlp_nll(int rows, const float *out, const float *target, const float *w, 
     tp::k_nll<<<(rows + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rows, out, target, w, inv_count, dout,
                                                                     loss_rows);
     return cuda_status(cudaGetLastError(), "mlp_nll launch");
+}
+
+int tp_mlp_pack(const float *W1, const float *W2, void *w1t, void *w2t, tp_stream_t stream)
+{
+    if (!W1 || !W2 || !w1t || !w2t) return fail(TP_ERR_ARG, "NULL mlp_pack operand");
+    if ((reinterpret_cast<uintptr_t>(w1t) | reinterpret_cast<uintptr_t>(w2t)) & 15)
+        return fail(TP_ERR_ARG, "packed weights must be 16-byte aligned");
+    int sms, rc;
+    if ((rc = sm_count(&sms))) return rc;
+    tp::k_mlp_pack<<<sms * 4, 256, 0, (cudaStream_t)stream>>>(W1, W2, static_cast<__nv_bfloat16 *>(w1t),
+                                                            static_cast<__nv_bfloat16 *>(w2t));
+    return cuda_status(cudaGetLastError(), "mlp_pack launch");
+}
+
+int tp_mlp_infer_tc(int rows, const float *x, int ldx, const void *w1t, const float *b1, const void *w2t,
+                    const float *b2, const float *W3, const float *b3, float *out, int *err, tp_stream_t stream)
+{
+    if (rows < 0 || ldx < 1350) return fail(TP_ERR_ARG, "mlp_infer rows %d ldx %d", rows, ldx);
+    if (!rows) return TP_OK;
+    if (!x || !w1t || !b1 || !w2t || !b2 || !W3 || !b3 || !out) return fail(TP_ERR_ARG, "NULL mlp_infer operand");
+    if (reinterpret_cast<uintptr_t>(w1t) & 15) return fail(TP_ERR_ARG, "w1t must be 16-byte aligned");
+    int sms, rc;
+    if ((rc = sm_count(&sms))) return rc;
+    if ((rc = set_smem_once(g_tc_attr, (const void *)tp::k_mlp_infer_tc, tp::kTcSmemBytes,
+                            "cudaFuncSetAttribute(k_mlp_infer_tc)")))
+        return rc;
+    const int tiles = (rows + tp::kTcM - 1) / tp::kTcM;
+    tp::k_mlp_infer_tc<<<tiles < sms ? tiles : sms, 128, tp::kTcSmemBytes, (cudaStream_t)stream>>>(
+        rows, x, ldx, static_cast<const __nv_bfloat16 *>(w1t), b1, static_cast<const __nv_bfloat16 *>(w2t), b2, W3,
+        b3, out, err);
+    return cuda_status(cudaGetLastError(), "mlp_infer_tc launch");
 }
 
 int tp_mlp_adam(size_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1, float beta2,

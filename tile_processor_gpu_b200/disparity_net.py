@@ -22,6 +22,7 @@ from . import _native
 from .api import _dptr, _stream
 
 N_IN, N_H1, N_H2, N_OUT = 1350, 256, 128, 2
+TC_KPAD = 1408  # layer-1 K of the tensor-core path (1350 padded to a multiple of 64)
 PARAMS = ("W1", "b1", "W2", "b2", "W3", "b3")
 SHAPES = {"W1": (N_IN, N_H1), "b1": (N_H1,), "W2": (N_H1, N_H2), "b2": (N_H2,), "W3": (N_H2, N_OUT),
           "b3": (N_OUT,)}
@@ -130,6 +131,25 @@ class DisparityMLP:
             _native.call("tp_mlp_adam", int(self.p[k].numel()), _dptr(self.p[k]), _dptr(self.g[k]),
                          _dptr(self.m[k]), _dptr(self.v[k]), float(lr), float(beta1), float(beta2), float(eps),
                          int(self.step_count), _stream(stream))
+
+    def pack(self, stream=None):
+        """W1^T and W2^T in BF16 for the tensor-core inference (after any update)."""
+        torch = _t()
+        if not hasattr(self, "w1t"):
+            self.w1t = torch.empty((N_H1, TC_KPAD), dtype=torch.bfloat16, device=self.device)
+            self.w2t = torch.empty((N_H2, N_H1), dtype=torch.bfloat16, device=self.device)
+            self.tc_err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        _native.call("tp_mlp_pack", _dptr(self.p["W1"]), _dptr(self.p["W2"]), _dptr(self.w1t), _dptr(self.w2t),
+                     _stream(stream))
+
+    def infer_tc(self, x, rows, out, ldx=N_IN, stream=None):
+        """out [rows][2] = (d, s) with layers 1-2 on the tensor cores (BF16
+        operands, FP32 accumulation); pack() must have run since the last update."""
+        p = self.p
+        _native.call("tp_mlp_infer_tc", int(rows), _dptr(x), int(ldx), _dptr(self.w1t), _dptr(p["b1"]),
+                     _dptr(self.w2t), _dptr(p["b2"]), _dptr(p["W3"]), _dptr(p["b3"]), _dptr(out), _dptr(self.tc_err),
+                     _stream(stream))
+        return out
 
     def host_params(self):
         return {k: v.cpu().numpy().copy() for k, v in self.p.items()}
