@@ -40,6 +40,7 @@ METRIC = "quad 5MP frames/s (CLT+corr+texture)"
 UNIT = "frames/s"
 CORR_RADIUS = 7
 DISPARITY_ERROR = 0.5
+LEARNED_LDX = 1352
 FAT_ZERO = 0.05
 TEXTURE = dict(colors=3, is_lwir=0, min_shot=10.0, scale_shot=3.0, diff_sigma=1.5, diff_threshold=10.0,
                min_agree=3.0, weight0=0.294118, weight1=0.117647, weight2=0.588235, dust_remove=1, keep_weights=0)
@@ -269,6 +270,25 @@ class FramePipeline:
         self.api.disparity_fit(self.g, self.corrs, self.corr_stride, CORR_RADIUS, self.num_corr, self.corr_idx,
                                self.port_offsets, self.disparity, self.strength)
 
+    def learned_setup(self):
+        """the shipped network (tile_processor_gpu_b200/data/disparity_mlp.npz), packed for the tensor cores"""
+        from tile_processor_gpu_b200 import disparity_net as D
+        torch = self.torch
+        path = os.path.join(ROOT, "tile_processor_gpu_b200", "data", "disparity_mlp.npz")
+        self.net = D.DisparityMLP.load(path, device=self.corrs.device)
+        self.net.pack()
+        # rows of 1352 floats start on 16-byte boundaries: 16-byte feature copies in the inference
+        self.feat = torch.zeros((self.TX * self.TY, LEARNED_LDX), dtype=torch.float32, device=self.corrs.device)
+        self.net_out = torch.zeros((self.TX * self.TY, 2), dtype=torch.float32, device=self.corrs.device)
+
+    def learned_features(self):
+        from tile_processor_gpu_b200 import disparity_net as D
+        D.features(self.g, self.corrs, self.corr_stride, CORR_RADIUS, self.num_corr, self.corr_idx, self.feat,
+                   feature_stride=LEARNED_LDX)
+
+    def learned_infer(self):
+        self.net.infer_tc(self.feat, self.TX * self.TY, self.net_out, ldx=LEARNED_LDX)
+
     def disparity_accuracy(self):
         """RMS error of the fitted residual against the truth on tiles whose
         footprint stays inside every camera's frame (disparity <= 64 px moves
@@ -278,10 +298,19 @@ class FramePipeline:
         inner = (tx >= 5) & (tx < self.TX - 5) & (ty >= 5) & (ty < self.TY - 5)
         got = self.disparity.cpu().numpy()[ty * self.TX + tx].astype(np.float64)
         res = got[inner] - self.true_residual[inner]
+        learned = None
+        if hasattr(self, "net_out"):
+            lg = got + self.net_out.cpu().numpy()[ty * self.TX + tx, 0].astype(np.float64)
+            lr = lg[inner] - self.true_residual[inner]
+            learned = {"rmse_px": round(float(np.sqrt(np.mean(lr ** 2))), 4),
+                       "outliers_gt_0.5px": round(float(np.mean(np.abs(lr) > 0.5)), 5),
+                       "net": "1350-256-128-2 GELU MLP on the six planes, shipped weights (4.87M synthetic "
+                              "tiles, 8 lenses), layer 1 TF32 and layer 2 BF16 tcgen05 MMAs (tp_mlp_infer_tc)"}
         return {"rmse_px": round(float(np.sqrt(np.mean(res ** 2))), 4),
                 "outliers_gt_0.5px": round(float(np.mean(np.abs(res) > 0.5)), 5),
                 "truth_rms_px": round(float(np.sqrt(np.mean(self.true_residual[inner] ** 2))), 4),
                 "tiles": int(inner.sum()), "fit": "3-point parabola on the 6-pair profile (tp_disparity_fit mode 0)",
+                "learned": learned,
                 "truth": "plane scene disparity; task error U[-%.1f, %.1f] px per tile" % (DISPARITY_ERROR,
                                                                                         DISPARITY_ERROR)}
 
@@ -399,8 +428,30 @@ def run_b200(args, rank, world, local, pg):
     d1.record(stream)
     torch.cuda.synchronize()
     fit_ms = d0.elapsed_time(d1) / fused_steps
+    # the learned residual on the same correlations: features and tensor-core inference
+    pipe.learned_setup()
+    pipe.learned_features()
+    pipe.learned_infer()
+    torch.cuda.synchronize()
+    l0, l1, l2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    l0.record(stream)
+    for _ in range(fused_steps):
+        pipe.learned_features()
+    l1.record(stream)
+    for _ in range(fused_steps):
+        pipe.learned_infer()
+    l2.record(stream)
+    torch.cuda.synchronize()
     disparity = pipe.disparity_accuracy()
     disparity["fit_ms"] = round(fit_ms, 4)
+    if disparity.get("learned"):
+        disparity["learned"]["features_ms"] = round(l0.elapsed_time(l1) / fused_steps, 4)
+        infer_ms = l1.elapsed_time(l2) / fused_steps
+        rows = pipe.TX * pipe.TY
+        disparity["learned"]["infer_ms"] = round(infer_ms, 4)
+        # algorithmic work of one inference: 2 (1350*256 + 256*128 + 128*2) flops and the 1350 FP32 features per row
+        disparity["learned"]["infer_tflops"] = round(rows * 2 * (1350 * 256 + 256 * 128 + 128 * 2) / infer_ms / 1e9, 1)
+        disparity["learned"]["infer_feature_gbs"] = round(rows * 1350 * 4 / infer_ms / 1e6, 1)
 
     # ---- end to end through the public API with host buffers ----
     # Every frame: its four images from pinned host memory to the device, the

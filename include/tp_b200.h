@@ -383,11 +383,15 @@ int tp_mlp_colsum(int rows, int cols, int ld, const float *x, float scale, float
 int tp_mlp_nll(int rows, const float *out, const float *target, const float *w, float inv_count, float *dout,
                float *loss_rows, tp_stream_t stream);
 /* Inference on the tensor cores: the weights packed once per update
- * (w1t: device uint16 [256][1408], W1^T in BF16, zero padded; w2t: device
- * uint16 [128][256], W2^T in BF16), then out[r] = {d, s} for feature rows x
- * (rows x 1350, leading dimension ldx), layers 1 and 2 as BF16 tcgen05 MMAs
- * with FP32 accumulation.  err (device int, may be NULL) is set to 1 if a
- * wait for the tensor cores ran out (no result then). */
+ * (w1t: device float [43 * 256 * 32], W1^T rounded to TF32 in 43 blocks of
+ * 32 rows of K, each block the shared-memory image of a tcgen05 B operand;
+ * w2t: device uint16 [128 * 256], W2^T in BF16, the same kind of image;
+ * both 16-byte aligned), then out[r] = {d, s} for feature rows x (rows x
+ * 1350, leading dimension ldx), layer 1 as TF32 and layer 2 as BF16 tcgen05
+ * MMAs with FP32 accumulation, the features fetched by TMA.  Rows of x must
+ * start on 16-byte boundaries (x 16-byte aligned, ldx a multiple of 4), else
+ * TP_ERR_ARG.  err (device int, may be NULL) is set to 1 if a wait for the
+ * copies or the tensor cores ran out (no result then). */
 int tp_mlp_pack(const float *W1, const float *W2, void *w1t, void *w2t, tp_stream_t stream);
 int tp_mlp_infer_tc(int rows, const float *x, int ldx, const void *w1t, const float *b1, const void *w2t,
                     const float *b2, const float *W3, const float *b3, float *out, int *err, tp_stream_t stream);

@@ -108,6 +108,13 @@ def test_rejects_bad_arguments(native):
     assert _code(lambda: N.call("tp_generate_RBGA_noalloc", big.ptr, fake, 4, 1024, 1024, fake, fake, *args, 0,
                                 8200, fake, None)) == N.TP_ERR_ARG
     assert "scratch" in N.last_error()
+    # tensor-core inference: feature rows must start on 16-byte boundaries (TMA strides)
+    for ldx, xp in ((1350, fake), (1353, fake), (1352, P(0x1004))):
+        assert _code(lambda: N.call("tp_mlp_infer_tc", 10, xp, ldx, fake, fake, fake, fake, fake, fake, fake, None,
+                                    None)) == N.TP_ERR_ARG
+        assert "16-byte" in N.last_error()
+    assert _code(lambda: N.call("tp_mlp_infer_tc", 10, fake, 1349, fake, fake, fake, fake, fake, fake, fake, None,
+                                None)) == N.TP_ERR_ARG
     # LPF table index
     v = np.zeros(64, np.float32)
     assert _code(lambda: N.call("tp_set_lpf", 6, v.ctypes.data_as(P))) == N.TP_ERR_ARG

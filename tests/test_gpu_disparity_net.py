@@ -132,13 +132,18 @@ def test_learned_residual_beats_plain_fit(native):
     assert hi > lo
 
 
-@pytest.mark.parametrize("rows", [200, 5000])
-def test_tensor_core_inference_matches_fp32(native, rows):
-    """tp_mlp_infer_tc (BF16 tcgen05 MMAs, FP32 accumulation) against the
-    FP32 forward pass: outputs within the BF16 rounding of the operands."""
+@pytest.mark.parametrize("rows,ldx", [(200, 1352), (5000, 1352), (40000, 1352), (40000, 1360), (300, 1356),
+                                      (129, 1352)])
+def test_tensor_core_inference_matches_fp32(native, rows, ldx):
+    """tp_mlp_infer_tc (TMA-fed TF32 layer 1, BF16 layer 2, FP32
+    accumulation) against the FP32 forward pass: outputs within the rounding
+    of the operands.  40000 rows give every CTA two or three tiles (the next
+    tile's first blocks load during the epilogues) and a ragged last tile;
+    129 rows a last tile of one row.  Columns past 1350 hold 1e30 and must not
+    reach the result (the tensor map ends at column 1350)."""
     import torch
     from tile_processor_gpu_b200 import disparity_net as D
-    rng = np.random.default_rng(rows)
+    rng = np.random.default_rng(rows + ldx)
     p = D.init_params(7)
     for k in p:
         if k.startswith("b"):
@@ -147,14 +152,18 @@ def test_tensor_core_inference_matches_fp32(native, rows):
     net = D.DisparityMLP(p)
     xd = _dev(x)
     ref = net.forward(xd, rows).clone()
+    xp = torch.full((rows, ldx), 1e30, dtype=torch.float32, device="cuda")
+    xp[:, :D.N_IN] = xd
     net.pack()
     out = torch.full((rows, 2), -99.0, device="cuda")
-    net.infer_tc(xd, rows, out)
+    net.infer_tc(xp, rows, out, ldx=ldx)
     torch.cuda.synchronize()
     assert int(net.tc_err.item()) == 0
     r, o = ref.cpu().numpy(), out.cpu().numpy()
+    assert np.all(np.isfinite(o))
     scale = np.abs(r).max(axis=0)
     err = np.abs(o - r).max(axis=0) / scale
-    print("\ntensor-core vs fp32, rows %d: max rel err %s" % (rows, err))
+    rms = np.sqrt(np.mean((o - r) ** 2)) / np.sqrt(np.mean(r ** 2))
+    print("\ntensor-core vs fp32, rows %d ldx %d: max rel err %s, rms rel %.2e" % (rows, ldx, err, rms))
     assert np.all(err < 3e-2)
-    assert np.sqrt(np.mean((o - r) ** 2)) / np.sqrt(np.mean(r ** 2)) < 1e-2
+    assert rms < 1e-2

@@ -6,6 +6,8 @@
  * stream.  Nothing here allocates, synchronises or copies device data to the
  * host.
  */
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <mutex>
@@ -149,6 +151,25 @@ int noalloc_scratch(int **out)
 /* host copy of the low-pass tables (last values set by tp_set_lpf) */
 float g_lpf_host[6][64] = TP_LPF_DEFAULT_INIT;
 const float g_lpf_default[6][64] = TP_LPF_DEFAULT_INIT;
+
+/* cuTensorMapEncodeTiled from the driver, looked up once */
+std::mutex g_tmap_mutex;
+PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
+
+int tensor_map_encoder(PFN_cuTensorMapEncodeTiled_v12000 *fn)
+{
+    std::lock_guard<std::mutex> lock(g_tmap_mutex);
+    if (!g_encode_tiled) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+            return fail(TP_ERR_CUDA, "cuTensorMapEncodeTiled not available (%s)", cudaGetErrorString(e));
+        g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    *fn = g_encode_tiled;
+    return TP_OK;
+}
 
 } /* namespace */
 
@@ -560,7 +581,7 @@ int tp_mlp_pack(const float *W1, const float *W2, void *w1t, void *w2t, tp_strea
         return fail(TP_ERR_ARG, "packed weights must be 16-byte aligned");
     int sms, rc;
     if ((rc = sm_count(&sms))) return rc;
-    tp::k_mlp_pack<<<sms * 4, 256, 0, (cudaStream_t)stream>>>(W1, W2, static_cast<__nv_bfloat16 *>(w1t),
+    tp::k_mlp_pack<<<sms * 4, 256, 0, (cudaStream_t)stream>>>(W1, W2, static_cast<float *>(w1t),
                                                             static_cast<__nv_bfloat16 *>(w2t));
     return cuda_status(cudaGetLastError(), "mlp_pack launch");
 }
@@ -571,16 +592,32 @@ int tp_mlp_infer_tc(int rows, const float *x, int ldx, const void *w1t, const fl
     if (rows < 0 || ldx < 1350) return fail(TP_ERR_ARG, "mlp_infer rows %d ldx %d", rows, ldx);
     if (!rows) return TP_OK;
     if (!x || !w1t || !b1 || !w2t || !b2 || !W3 || !b3 || !out) return fail(TP_ERR_ARG, "NULL mlp_infer operand");
-    if (reinterpret_cast<uintptr_t>(w1t) & 15) return fail(TP_ERR_ARG, "w1t must be 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(w1t) | reinterpret_cast<uintptr_t>(w2t)) & 15)
+        return fail(TP_ERR_ARG, "w1t / w2t must be 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(x) & 15) || (ldx & 3))
+        return fail(TP_ERR_ARG, "feature rows must start on 16-byte boundaries (x aligned, ldx %d a multiple of 4)",
+                    ldx);
     int sms, rc;
     if ((rc = sm_count(&sms))) return rc;
+    PFN_cuTensorMapEncodeTiled_v12000 encode;
+    if ((rc = tensor_map_encoder(&encode))) return rc;
+    /* the features as a 2-D FP32 tensor of 1350 x rows, boxes of 32 x 128 with 128-byte swizzle */
+    CUtensorMap tmap;
+    const cuuint64_t dims[2] = {1350, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldx * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)tp::kTcKB, (cuuint32_t)tp::kTcM};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult cr = encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(x), dims, strides, box,
+                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return fail(TP_ERR_ARG, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
     if ((rc = set_smem_once(g_tc_attr, (const void *)tp::k_mlp_infer_tc, tp::kTcSmemBytes,
                             "cudaFuncSetAttribute(k_mlp_infer_tc)")))
         return rc;
     const int tiles = (rows + tp::kTcM - 1) / tp::kTcM;
     tp::k_mlp_infer_tc<<<tiles < sms ? tiles : sms, 128, tp::kTcSmemBytes, (cudaStream_t)stream>>>(
-        rows, x, ldx, static_cast<const __nv_bfloat16 *>(w1t), b1, static_cast<const __nv_bfloat16 *>(w2t), b2, W3,
-        b3, out, err);
+        tmap, rows, static_cast<const float *>(w1t), b1, static_cast<const __nv_bfloat16 *>(w2t), b2, W3, b3, out,
+        err);
     return cuda_status(cudaGetLastError(), "mlp_infer_tc launch");
 }
 

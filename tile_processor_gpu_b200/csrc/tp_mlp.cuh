@@ -19,6 +19,7 @@
  * Adam.  Rows are samples; matrices are row-major with leading dimensions.
  */
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "tp_common.cuh"
@@ -213,39 +214,64 @@ __global__ void k_adam(long long n, float *__restrict__ p, const float *__restri
 
 
 
-/* ---- inference on the tensor cores (tcgen05) -------------------------------
+/* ---- inference on the tensor cores (tcgen05 + TMA) --------------------------
  *
- * out[r] = the network at feature row r, layers 1 and 2 as BF16 x BF16 -> FP32
- * tcgen05 MMAs with the accumulators in tensor memory, layer 3 and the
- * activations on the CUDA cores.  Persistent: one 128-thread CTA per SM walks
- * 128-row tiles.  Per tile:
- *   layer 1: for each 64-wide K block, the features (FP32 -> BF16) and W1^T
- *     (packed BF16) are written to shared memory in the canonical K-major,
- *     non-swizzled layout (8-row x 16-byte core matrices; the 16-byte K chunks
- *     LBO apart, 8-row groups 128 bytes apart); one thread issues four
- *     M=128, N=256, K=16 MMAs into TMEM columns 0..255 and commits them to an
- *     mbarrier that every thread waits on (bounded) before the next block;
- *   epilogue 1: warp w reads its 32 rows (TMEM lanes 32w..) in 8-column
- *     pieces, adds b1, applies GELU and writes BF16 rows of H1 to shared
- *     memory in the same layout -- the A operand of layer 2;
- *   layer 2: sixteen M=128, N=128, K=16 MMAs against W2^T (loaded once per
- *     CTA) into TMEM columns 256..383;
- *   epilogue 2: + b2, GELU, then layer 3 (128 -> 2) per row in registers.
- * A wait that runs out sets *err and the CTA stops after freeing its TMEM.
+ * out[r] = the network at feature row r: layer 1 as TF32 x TF32 -> FP32 and
+ * layer 2 as BF16 x BF16 -> FP32 tcgen05 MMAs with the accumulators in tensor
+ * memory (columns 0..255 and 256..383), layer 3 and the activations on the
+ * CUDA cores.  Persistent: one 128-thread CTA per SM walks 128-row tiles.
+ *
+ * Layer 1 runs over 43 K blocks of 32 through a three-stage ring of shared
+ * memory.  Thread 32 is the producer: per block one TMA tensor load of the
+ * 128 x 32 FP32 feature box (128-byte swizzle; columns past 1349 and rows past
+ * `rows` arrive as zeros) and one bulk copy of the 32 KB W1^T block, which
+ * k_mlp_pack stores already in the canonical K-major, non-swizzled image
+ * (8-row x 16-byte core matrices, K chunks 4096 bytes apart), both completing
+ * on the stage's `full` mbarrier.  Thread 0 issues the block's four M=128,
+ * N=256, K=8 MMAs once `full` flips and commits them to the stage's `empty`
+ * mbarrier, which the producer waits on before refilling the stage; after
+ * the last block it commits `acc`.  The other threads wait on `acc`.
+ * Epilogue 1: warp w reads its 32 rows (TMEM lanes 32w..) in 32-column pieces,
+ * adds b1, applies GELU and writes BF16 rows of H1 over the first 64 KB of the
+ * ring (stages 0 and 1); block kb of every tile uses stage (kb + 2) % 3, so the
+ * next tile's block 0 (stage 2) is loading meanwhile.  Layer 2: sixteen
+ * M=128, N=128, K=16 MMAs against W2^T (one bulk copy per CTA, also stored
+ * pre-laid-out) committed to `l2`; once it flips the next tile's block 1 may
+ * overwrite stage 0.  Epilogue 2: + b2, GELU, layer 3 (128 -> 2) per row.
+ * Every commit and every load completion is waited exactly once, in order,
+ * so one parity bit per mbarrier tracks its phase.  A wait that runs out
+ * makes its thread stop issuing; the CTA leaves the loop together at the next
+ * barrier, waits (bounded) for its copies and MMAs in flight, sets *err and
+ * frees its TMEM.
  */
-constexpr int kTcM = 128, kTcK = 64, kTcN1 = 256, kTcN2 = 128;
-constexpr int kTcKPad = 1408;                        /* 1350 padded to a multiple of 64 */
-constexpr int kTcBytesA = kTcM * kTcK * 2;           /* features block, 16 KB          */
-constexpr int kTcBytesB1 = kTcN1 * kTcK * 2;         /* W1^T block, 32 KB              */
-constexpr int kTcBytesH1 = kTcM * kTcN1 * 2;         /* H1, 64 KB                      */
-constexpr int kTcBytesW2 = kTcN2 * kTcN1 * 2;        /* W2^T, 64 KB                    */
-constexpr int kTcSmemBytes = 1024 + kTcBytesA + kTcBytesB1 + kTcBytesH1 + kTcBytesW2 +
-                             4 * (kTcN1 + kTcN2 + 2 * kTcN2 + 2) + 128;
+constexpr int kTcM = 128, kTcN1 = 256, kTcN2 = 128;
+constexpr int kTcKB = 32;                         /* TF32 elements of K per block    */
+constexpr int kTcBlocks = 43;                     /* 1350 -> 1376 = 43 x 32          */
+constexpr int kTcKPad = kTcBlocks * kTcKB;
+constexpr int kTcStages = 3;
+constexpr int kTcBytesA = kTcM * kTcKB * 4;       /* feature box, 16 KB              */
+constexpr int kTcBytesB1 = kTcN1 * kTcKB * 4;     /* W1^T block, 32 KB               */
+constexpr int kTcBytesStage = kTcBytesA + kTcBytesB1;
+constexpr int kTcBytesRing = kTcStages * kTcBytesStage; /* 144 KB                   */
+constexpr int kTcBytesH1 = kTcM * kTcN1 * 2;      /* H1 in BF16, 64 KB, over stages 0-1 */
+constexpr int kTcBytesW2 = kTcN2 * kTcN1 * 2;     /* W2^T in BF16, 64 KB             */
+static_assert(kTcBytesH1 <= 2 * kTcBytesStage, "H1 must stay clear of stage 2");
+static_assert(kTcBytesStage % 1024 == 0, "stages start on 1024-byte boundaries (128-byte swizzle)");
+static_assert(kTcKPad >= 1350 && kTcKPad - kTcKB < 1350, "K blocking");
+constexpr int kTcTableFloats = kTcN1 + kTcN2 + 2 * kTcN2 + 2;
+enum { kBarFull = 0, kBarEmpty = 3, kBarAcc = 6, kBarL2 = 7, kBarW2 = 8, kBarDrain = 9, kTcBars = 10 };
+constexpr int kTcSmemBytes = 1024 + kTcBytesRing + kTcBytesW2 + 4 * kTcTableFloats + 8 * kTcBars + 64;
 
-/* byte offset of element (row r, k) in a canonical K-major block of `rows` rows */
-__device__ __forceinline__ uint32_t tc_off(int r, int k, int rows)
+/* byte offset of BF16 element (row r, k) in a canonical K-major block of `rows` rows */
+__host__ __device__ constexpr uint32_t tc_off(int r, int k, int rows)
 {
     return (uint32_t)((k >> 3) * (rows / 8) * 128 + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+/* byte offset of TF32 element (row r, k) in a canonical K-major block of `rows` rows */
+__host__ __device__ constexpr uint32_t tc_off32(int r, int k, int rows)
+{
+    return (uint32_t)((k >> 2) * (rows / 8) * 128 + (r >> 3) * 128 + (r & 7) * 16 + (k & 3) * 4);
 }
 
 /* shared-memory matrix descriptor: no swizzle, K-major, version 1 */
@@ -255,16 +281,32 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32
            ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-/* instruction descriptor: BF16 x BF16 -> F32, both K-major, M x N */
-__host__ __device__ constexpr uint32_t tc_idesc(int M, int N)
+/* K-major, 128-byte swizzle: rows of 128 bytes, 8-row groups 1024 bytes apart
+ * (SBO), LBO unused (1); layout type 2 */
+__device__ __forceinline__ uint64_t tc_desc_sw128(uint32_t saddr)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+
+/* instruction descriptor: FP32 accumulator, A and B both of format `fmt`
+ * (1 = BF16 for kind::f16, 2 = TF32 for kind::tf32), both K-major, M x N */
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N, uint32_t fmt = 1u)
+{
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
 {
     asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+                 "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void tc_mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
                  "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
@@ -289,15 +331,47 @@ __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity)
     return false;
 }
 
-__device__ __forceinline__ void tc_ld8(uint32_t taddr, float v[8])
+/* the producer's arrival on a `full` mbarrier, announcing `bytes` of copies */
+__device__ __forceinline__ void tc_expect(uint32_t mbar, uint32_t bytes)
 {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(mbar),
+                 "r"(bytes)
+                 : "memory");
+}
+
+/* 2-D TMA tensor load of the box at (x, y) (elements) into shared memory */
+__device__ __forceinline__ void tc_tma_load_2d(uint32_t dst, const void *tmap, int x, int y, uint32_t mbar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                 "[%4];" ::"r"(dst),
+                 "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(mbar)
+                 : "memory");
+}
+
+/* bulk copy of `bytes` (multiple of 16, both ends 16-byte aligned) into shared memory */
+__device__ __forceinline__ void tc_bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+
+/* 32 consecutive TMEM columns of this thread's lane, one wait */
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float v[32])
+{
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                 "[%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                   "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                  : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
@@ -307,61 +381,68 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
     return lo | (hi << 16);
 }
 
-/* W1 [1350][256] -> W1^T BF16 [256][1408] (zero padded); W2 [256][128] ->
- * W2^T BF16 [128][256] */
-__global__ void k_mlp_pack(const float *__restrict__ W1, const float *__restrict__ W2,
-                           __nv_bfloat16 *__restrict__ w1t, __nv_bfloat16 *__restrict__ w2t)
+/* FP32 -> TF32 (round to nearest, ties away; low 13 bits zero) */
+__device__ __forceinline__ float to_tf32(float x)
 {
-    const int n1 = kTcN1 * kTcKPad, n2 = kTcN2 * kTcN1;
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+/* W1 [1350][256] -> 43 blocks of 256 x 32 TF32 (W1^T, zero past row 1349),
+ * each the byte image of a canonical non-swizzled K-major B operand;
+ * W2 [256][128] -> the image of W2^T in BF16 (128 x 256, same layout) */
+__global__ void k_mlp_pack(const float *__restrict__ W1, const float *__restrict__ W2, float *__restrict__ w1img,
+                           __nv_bfloat16 *__restrict__ w2img)
+{
+    const int n1 = kTcBlocks * kTcN1 * kTcKB, n2 = kTcN2 * kTcN1;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1 + n2; i += gridDim.x * blockDim.x) {
         if (i < n1) {
-            const int n = i / kTcKPad, k = i - n * kTcKPad;
-            w1t[i] = __float2bfloat16_rn(k < 1350 ? W1[(size_t)k * kTcN1 + n] : 0.0f);
+            const int kb = i / (kTcN1 * kTcKB), e = i - kb * (kTcN1 * kTcKB);
+            const int n = e / kTcKB, kk = e - n * kTcKB, k = kb * kTcKB + kk;
+            w1img[(size_t)kb * (kTcN1 * kTcKB) + tc_off32(n, kk, kTcN1) / 4] =
+                k < 1350 ? to_tf32(W1[(size_t)k * kTcN1 + n]) : 0.0f;
         } else {
             const int j = i - n1, n = j / kTcN1, k = j - n * kTcN1;
-            w2t[j] = __float2bfloat16_rn(W2[(size_t)k * kTcN2 + n]);
+            w2img[tc_off(n, k, kTcN2) / 2] = __float2bfloat16_rn(W2[(size_t)k * kTcN2 + n]);
         }
     }
 }
 
-__global__ void __launch_bounds__(128, 1) k_mlp_infer_tc(int rows, const float *__restrict__ x, int ldx,
-                                                         const __nv_bfloat16 *__restrict__ w1t,
+__global__ void __launch_bounds__(128, 1) k_mlp_infer_tc(const __grid_constant__ CUtensorMap tmap_x, int rows,
+                                                         const float *__restrict__ w1img,
                                                          const float *__restrict__ b1,
-                                                         const __nv_bfloat16 *__restrict__ w2t,
+                                                         const __nv_bfloat16 *__restrict__ w2img,
                                                          const float *__restrict__ b2,
                                                          const float *__restrict__ W3,
                                                          const float *__restrict__ b3, float *__restrict__ out,
                                                          int *__restrict__ err)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
-    /* 1024-byte aligned operand buffers, then the small tables */
+    /* 1024-byte aligned ring (H1 over its start), W2^T, then the small tables */
     const uint32_t base_s = (uint32_t)__cvta_generic_to_shared(tc_smem);
     const uint32_t pad = (1024 - (base_s & 1023)) & 1023;
     unsigned char *sm = tc_smem + pad;
-    unsigned char *sA = sm, *sB1 = sA + kTcBytesA, *sH1 = sB1 + kTcBytesB1, *sW2 = sH1 + kTcBytesH1;
-    float *sb1 = reinterpret_cast<float *>(sW2 + kTcBytesW2);
+    unsigned char *sH1 = sm;
+    float *sb1 = reinterpret_cast<float *>(sm + kTcBytesRing + kTcBytesW2);
     float *sb2 = sb1 + kTcN1, *sW3 = sb2 + kTcN2, *sb3 = sW3 + 2 * kTcN2;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(sb3 + 2) + 1; /* 8-byte aligned */
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 1);
-    const uint32_t aA = (uint32_t)__cvta_generic_to_shared(sA), aB1 = (uint32_t)__cvta_generic_to_shared(sB1);
-    const uint32_t aH1 = (uint32_t)__cvta_generic_to_shared(sH1), aW2 = (uint32_t)__cvta_generic_to_shared(sW2);
-    const uint32_t aMbar = (uint32_t)__cvta_generic_to_shared(mbar);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sb3 + 2);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + kTcBars);
+    const uint32_t aRing = base_s + pad, aH1 = aRing, aW2 = aRing + kTcBytesRing;
+    const uint32_t aBar = (uint32_t)__cvta_generic_to_shared(mbar);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    /* tables and W2^T (K-major, 128 rows of N) once per CTA */
+    const bool producer = tid == 32, issuer = tid == 0;
     for (int i = tid; i < kTcN1; i += 128) sb1[i] = b1[i];
     for (int i = tid; i < kTcN2; i += 128) sb2[i] = b2[i];
     for (int i = tid; i < 2 * kTcN2; i += 128) sW3[i] = W3[i];
     if (tid < 2) sb3[tid] = b3[tid];
-    for (int i = tid; i < kTcN2 * kTcN1 / 2; i += 128) {
-        const int n = (2 * i) / kTcN1, k = (2 * i) - n * kTcN1;
-        const uint32_t v = *reinterpret_cast<const uint32_t *>(w2t + (size_t)n * kTcN1 + k);
-        *reinterpret_cast<uint32_t *>(sW2 + tc_off(n, k, kTcN2)) = v;
-    }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(aMbar) : "memory");
+    if (issuer) {
+        for (int b = 0; b < kTcBars; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(aBar + 8 * b) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (producer) asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap_x)) : "memory");
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
                          (uint32_t)__cvta_generic_to_shared(tmem_slot))
@@ -372,91 +453,128 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer_tc(int rows, const float *
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-    uint32_t phase = 0;
-    bool ok = true;
-    const uint32_t idesc1 = tc_idesc(kTcM, kTcN1), idesc2 = tc_idesc(kTcM, kTcN2);
+    const uint32_t idesc1 = tc_idesc(kTcM, kTcN1, 2u), idesc2 = tc_idesc(kTcM, kTcN2, 1u);
     const int tiles = (rows + kTcM - 1) / kTcM;
+    auto stage_of = [](int kb) { return (kb + 2) % kTcStages; };
+    auto sA = [&](int s) { return aRing + (uint32_t)(s * kTcBytesStage); };
+    auto sB = [&](int s) { return aRing + (uint32_t)(s * kTcBytesStage + kTcBytesA); };
+    auto bar = [&](int b) { return aBar + 8u * (uint32_t)b; };
 
-    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-        const int r0 = t * kTcM;
+    bool ok = true;          /* this thread's waits so far */
+    bool failed = false;     /* CTA-uniform */
+    uint32_t ph = 0;         /* parity bit per mbarrier, this thread's view */
+    int nload[kTcStages] = {0, 0, 0}; /* producer: loads issued per stage */
+    bool w2_issued = false;
+    auto wait_bar = [&](int b) {
+        if (ok) ok = tc_wait(bar(b), (ph >> b) & 1u);
+        ph ^= 1u << b;
+    };
+    auto load_block = [&](int tile, int kb) {
+        const int s = stage_of(kb);
+        tc_expect(bar(kBarFull + s), (uint32_t)kTcBytesStage);
+        tc_tma_load_2d(sA(s), &tmap_x, kb * kTcKB, tile * kTcM, bar(kBarFull + s));
+        tc_bulk_load(sB(s), w1img + (size_t)kb * (kTcN1 * kTcKB), (uint32_t)kTcBytesB1, bar(kBarFull + s));
+        nload[s]++;
+    };
+
+    int t = blockIdx.x;
+    if (producer && t < tiles) {
+        tc_expect(bar(kBarW2), (uint32_t)kTcBytesW2);
+        tc_bulk_load(aW2, w2img, (uint32_t)kTcBytesW2, bar(kBarW2));
+        w2_issued = true;
+        load_block(t, 0);
+        load_block(t, 1);
+    }
+    bool first = true;
+    for (; t < tiles; t += gridDim.x) {
+        const int r0 = t * kTcM, tn = t + (int)gridDim.x;
         /* ---- layer 1 ---- */
-        for (int kb = 0; kb < kTcKPad / kTcK && ok; kb++) {
-            const int k0 = kb * kTcK;
-            /* features: warp w rows 32w..32w+31, lane = k pair */
-            for (int rr = 0; rr < 32; rr++) {
-                const int r = warp * 32 + rr, gr = r0 + r, k = k0 + 2 * lane;
-                float2 v = make_float2(0.0f, 0.0f);
-                if (gr < rows) {
-                    const float *px = x + (size_t)gr * ldx + k;
-                    if (k < 1350) v.x = px[0];
-                    if (k + 1 < 1350) v.y = px[1];
-                }
-                *reinterpret_cast<uint32_t *>(sA + tc_off(r, 2 * lane, kTcM)) = pack_bf16(v.x, v.y);
+        if (producer) {
+            for (int kb = 2; kb < kTcBlocks && ok; kb++) {
+                if (kb >= 3) wait_bar(kBarEmpty + stage_of(kb)); /* MMAs of block kb - 3 */
+                if (ok) load_block(t, kb);
             }
-            /* W1^T block: 256 rows x 64 k, 16 bytes (8 k) per thread-step */
-            for (int i = tid; i < kTcN1 * (kTcK / 8); i += 128) {
-                const int n = i >> 3, kc = i & 7;
-                const uint4 v = *reinterpret_cast<const uint4 *>(w1t + (size_t)n * kTcKPad + k0 + kc * 8);
-                *reinterpret_cast<uint4 *>(sB1 + tc_off(n, kc * 8, kTcN1)) = v;
-            }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (tid == 0) {
+            /* the last three blocks' MMAs, in commit order */
+            for (int kb = kTcBlocks - 3; kb < kTcBlocks; kb++) wait_bar(kBarEmpty + stage_of(kb));
+            if (ok && tn < tiles) load_block(tn, 0); /* stage 2: clear of H1 */
+        } else if (issuer) {
+            for (int kb = 0; kb < kTcBlocks && ok; kb++) {
+                const int s = stage_of(kb);
+                wait_bar(kBarFull + s);
+                if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-                for (int j = 0; j < kTcK / 16; j++) {
-                    const uint64_t da = tc_desc(aA + j * 2 * (kTcM / 8) * 128, (kTcM / 8) * 128, 128);
-                    const uint64_t db = tc_desc(aB1 + j * 2 * (kTcN1 / 8) * 128, (kTcN1 / 8) * 128, 128);
-                    tc_mma(tmem, da, db, idesc1, (kb > 0 || j > 0) ? 1u : 0u);
+                for (int j = 0; j < kTcKB / 8; j++) {
+                    const uint64_t da = tc_desc_sw128(sA(s) + 32u * j);
+                    const uint64_t db = tc_desc(sB(s) + j * 2 * (kTcN1 / 8) * 128, (kTcN1 / 8) * 128, 128);
+                    tc_mma_tf32(tmem, da, db, idesc1, (kb > 0 || j > 0) ? 1u : 0u);
                 }
-                tc_commit(aMbar);
+                tc_commit(bar(kBarEmpty + s));
             }
-            /* every thread takes the same branch after a wait */
-            ok = __syncthreads_and(tc_wait(aMbar, phase) ? 1 : 0) != 0;
-            phase ^= 1u;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (ok) tc_commit(bar(kBarAcc));
         }
-        if (!ok) break;
+        __syncwarp();
+        wait_bar(kBarAcc);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!__syncthreads_and(ok ? 1 : 0)) {
+            failed = true;
+            break;
+        }
+        __syncwarp();
         /* ---- epilogue 1: H1 = gelu(D1 + b1) as BF16 rows of the layer-2 A operand ---- */
         {
             const int r = warp * 32 + lane;
-            for (int c0 = 0; c0 < kTcN1; c0 += 8) {
-                float v[8];
-                tc_ld8(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
-                uint32_t w[4];
+            for (int c0 = 0; c0 < kTcN1; c0 += 32) {
+                float v[32];
+                tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
 #pragma unroll
-                for (int i = 0; i < 4; i++)
-                    w[i] = pack_bf16(gelu_f(v[2 * i] + sb1[c0 + 2 * i]), gelu_f(v[2 * i + 1] + sb1[c0 + 2 * i + 1]));
-                *reinterpret_cast<uint4 *>(sH1 + tc_off(r, c0, kTcM)) = make_uint4(w[0], w[1], w[2], w[3]);
+                for (int q = 0; q < 4; q++) {
+                    uint32_t w[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const int c = c0 + 8 * q + 2 * i;
+                        w[i] = pack_bf16(gelu_f(v[8 * q + 2 * i] + sb1[c]), gelu_f(v[8 * q + 2 * i + 1] + sb1[c + 1]));
+                    }
+                    *reinterpret_cast<uint4 *>(sH1 + tc_off(r, c0 + 8 * q, kTcM)) = make_uint4(w[0], w[1], w[2], w[3]);
+                }
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         /* ---- layer 2 ---- */
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (issuer) {
+            if (first) wait_bar(kBarW2);
+            if (ok) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-            for (int j = 0; j < kTcN1 / 16; j++) {
-                const uint64_t da = tc_desc(aH1 + j * 2 * (kTcM / 8) * 128, (kTcM / 8) * 128, 128);
-                const uint64_t db = tc_desc(aW2 + j * 2 * (kTcN2 / 8) * 128, (kTcN2 / 8) * 128, 128);
-                tc_mma(tmem + kTcN1, da, db, idesc2, j > 0 ? 1u : 0u);
+                for (int j = 0; j < kTcN1 / 16; j++) {
+                    const uint64_t da = tc_desc(aH1 + j * 2 * (kTcM / 8) * 128, (kTcM / 8) * 128, 128);
+                    const uint64_t db = tc_desc(aW2 + j * 2 * (kTcN2 / 8) * 128, (kTcN2 / 8) * 128, 128);
+                    tc_mma(tmem + kTcN1, da, db, idesc2, j > 0 ? 1u : 0u);
+                }
+                tc_commit(bar(kBarL2));
             }
-            tc_commit(aMbar);
         }
-        ok = __syncthreads_and(tc_wait(aMbar, phase) ? 1 : 0) != 0;
-        phase ^= 1u;
+        first = false;
+        __syncwarp();
+        wait_bar(kBarL2);
+        /* H1 consumed: the next tile's block 1 may overwrite stage 0 */
+        if (producer && ok && tn < tiles) load_block(tn, 1);
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (!ok) break;
+        if (!__syncthreads_and(ok ? 1 : 0)) {
+            failed = true;
+            break;
+        }
         /* ---- epilogue 2 and layer 3 ---- */
         {
             const int r = warp * 32 + lane, gr = r0 + r;
             float o0 = sb3[0], o1 = sb3[1];
-            for (int c0 = 0; c0 < kTcN2; c0 += 8) {
-                float v[8];
-                tc_ld8(tmem + ((uint32_t)(warp * 32) << 16) + kTcN1 + c0, v);
+            for (int c0 = 0; c0 < kTcN2; c0 += 32) {
+                float v[32];
+                tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + kTcN1 + c0, v);
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
+                for (int i = 0; i < 32; i++) {
                     const float h = gelu_f(v[i] + sb2[c0 + i]);
                     o0 = __fmaf_rn(h, sW3[2 * (c0 + i)], o0);
                     o1 = __fmaf_rn(h, sW3[2 * (c0 + i) + 1], o1);
@@ -467,12 +585,25 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer_tc(int rows, const float *
                 out[2 * (size_t)gr + 1] = o1;
             }
         }
+        /* TMEM columns 256.. are rewritten only after the next tile's layer 1 */
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads(); /* H1 and TMEM free for the next tile */
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
-    if (!ok && tid == 0 && err) atomicExch(err, 1);
+    if (failed) {
+        /* copies still in flight land before the CTA exits; MMAs get one more bounded wait */
+        if (producer) {
+            for (int s = 0; s < kTcStages; s++)
+                if (nload[s] > 0) (void)tc_wait(bar(kBarFull + s), (uint32_t)(nload[s] - 1) & 1u);
+            if (w2_issued) (void)tc_wait(bar(kBarW2), 0u);
+        }
+        if (issuer) {
+            tc_commit(bar(kBarDrain));
+            (void)tc_wait(bar(kBarDrain), 0u);
+            if (err) atomicExch(err, 1);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
 }

@@ -22,7 +22,8 @@ from . import _native
 from .api import _dptr, _stream
 
 N_IN, N_H1, N_H2, N_OUT = 1350, 256, 128, 2
-TC_KPAD = 1408  # layer-1 K of the tensor-core path (1350 padded to a multiple of 64)
+TC_KPAD = 1376  # layer-1 K of the tensor-core path (1350 padded to 43 blocks of 32)
+TC_LDX = 1352  # feature rows on 16-byte boundaries, as the tensor-core inference needs
 PARAMS = ("W1", "b1", "W2", "b2", "W3", "b3")
 SHAPES = {"W1": (N_IN, N_H1), "b1": (N_H1,), "W2": (N_H1, N_H2), "b2": (N_H2,), "W3": (N_H2, N_OUT),
           "b3": (N_OUT,)}
@@ -63,6 +64,15 @@ def features(geom, corrs, corr_stride, corr_radius, num_corr, corr_indices, out,
     """Rows out[tile] of the tiles with correlation entries (others untouched)."""
     _native.call("tp_mlp_features", geom.ptr, _dptr(corrs), int(corr_stride), int(corr_radius), int(num_corr),
                  _dptr(corr_indices), _dptr(out), int(feature_stride), _stream(stream))
+
+
+def pad_rows(x, ldx=TC_LDX):
+    """Copy of feature rows x [rows][>= 1350] with leading dimension ldx
+    (zeros past column 1349), for the tensor-core inference."""
+    torch = _t()
+    out = torch.zeros((x.shape[0], ldx), dtype=torch.float32, device=x.device)
+    out[:, :N_IN] = x[:, :N_IN]
+    return out
 
 
 class DisparityMLP:
@@ -133,18 +143,20 @@ class DisparityMLP:
                          int(self.step_count), _stream(stream))
 
     def pack(self, stream=None):
-        """W1^T and W2^T in BF16 for the tensor-core inference (after any update)."""
+        """W1^T in TF32 and W2^T in BF16 for the tensor-core inference (after any update)."""
         torch = _t()
         if not hasattr(self, "w1t"):
-            self.w1t = torch.empty((N_H1, TC_KPAD), dtype=torch.bfloat16, device=self.device)
+            self.w1t = torch.empty((N_H1, TC_KPAD), dtype=torch.float32, device=self.device)
             self.w2t = torch.empty((N_H2, N_H1), dtype=torch.bfloat16, device=self.device)
             self.tc_err = torch.zeros(1, dtype=torch.int32, device=self.device)
         _native.call("tp_mlp_pack", _dptr(self.p["W1"]), _dptr(self.p["W2"]), _dptr(self.w1t), _dptr(self.w2t),
                      _stream(stream))
 
-    def infer_tc(self, x, rows, out, ldx=N_IN, stream=None):
-        """out [rows][2] = (d, s) with layers 1-2 on the tensor cores (BF16
-        operands, FP32 accumulation); pack() must have run since the last update."""
+    def infer_tc(self, x, rows, out, ldx=TC_LDX, stream=None):
+        """out [rows][2] = (d, s) with layers 1-2 on the tensor cores (TF32 and
+        BF16 operands, FP32 accumulation); pack() must have run since the last
+        update.  Rows of x must start on 16-byte boundaries (ldx a multiple of
+        4): see pad_rows."""
         p = self.p
         _native.call("tp_mlp_infer_tc", int(rows), _dptr(x), int(ldx), _dptr(self.w1t), _dptr(p["b1"]),
                      _dptr(self.w2t), _dptr(p["b2"]), _dptr(p["W3"]), _dptr(p["b3"]), _dptr(out), _dptr(self.tc_err),
