@@ -106,6 +106,45 @@ def test_features(native):
     assert np.all(got[~seen] == -5.0)
 
 
+def test_features_irregular_runs(native):
+    """Runs the register path does not take: a pair listed twice (the later
+    plane is kept, both count in the maximum), pair codes >= 6 (skipped) and
+    a run of 40 entries; ordinary runs beside them."""
+    import torch
+    from tile_processor_gpu_b200 import api, disparity_net as D, synth
+    geom = synth.geometry(128, 128)
+    g = api.Geometry.from_dict(geom)
+    TX, TY, _ = synth.tiles(geom)
+    rng = np.random.default_rng(5)
+    codes = []
+    codes += [(3 << 8) | p for p in (0, 1, 2, 1)]                 # pair 1 twice
+    codes += [(4 << 8) | p for p in (0, 6, 7, 5)]                 # codes 6, 7 skipped
+    codes += [(5 << 8) | (i % 6) for i in range(40)]              # 40 entries
+    codes += [(6 << 8) | p for p in (0, 1, 2, 3, 4, 5)]           # ordinary
+    codes += [(7 << 8) | 2]                                       # one entry
+    idx = np.array(codes, np.int32)
+    stride = 230
+    co = rng.normal(0, 1, (len(idx), stride)).astype(np.float32)
+    co[len(idx) - 1, :225] *= 50.0
+    feat = torch.full((TX * TY, D.N_IN), -5.0, device="cuda")
+    D.features(g, torch.from_numpy(co).cuda(), stride, 7, len(idx), torch.from_numpy(idx).cuda(), feat)
+    torch.cuda.synchronize()
+    got = feat.cpu().numpy()
+    for tile in (3, 4, 5, 6, 7):
+        want = np.zeros(D.N_IN, np.float64)
+        mx = 0.0
+        for e, code in enumerate(idx):
+            if code >> 8 != tile or (code & 0xFF) >= 6:
+                continue
+            p = code & 0xFF
+            want[p * 225:(p + 1) * 225] = co[e, :225]
+            mx = max(mx, float(np.abs(co[e, :225]).max()))
+        np.testing.assert_allclose(got[tile], want / mx, rtol=0, atol=1e-6)
+    untouched = np.ones(TX * TY, bool)
+    untouched[[3, 4, 5, 6, 7]] = False
+    assert np.all(got[untouched] == -5.0)
+
+
 def test_learned_residual_beats_plain_fit(native):
     """Trained on eight synthetic frames, on a held-out frame the network's
     estimate (plain fit + correction) has a smaller RMS error against the

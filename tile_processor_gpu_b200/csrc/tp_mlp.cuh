@@ -31,18 +31,62 @@ namespace tp {
 /* One warp per correlation entry; the warp holding the first entry of a
  * tile's run (entries of one tile adjacent) writes the tile's row:
  * feat[tile][p * n2 + k] = C_p[k] / max |C| over the run, zeros for pairs the
- * run does not list. */
+ * run does not list (a pair listed twice: the later entry's plane, both in
+ * the maximum; entries with p >= 6 are skipped).  The warp reads idx[e ..
+ * e + 31] at once to find the run; a run of at most 32 entries without a
+ * repeated pair is read once into registers (lane l holds k = l + 32 i of
+ * every pair) and written once; other runs take the two-pass loop. */
 __global__ void __launch_bounds__(256) k_mlp_features(int ntiles, const float *__restrict__ corrs,
                                                       size_t corr_stride, int n2, long long num,
                                                       const int *__restrict__ idx, float *__restrict__ feat,
                                                       size_t feat_stride)
 {
+    constexpr int kPer = 8; /* ceil(225 / 32): n2 <= 225 */
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
     for (long long e = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < num; e += warps) {
         const int tile = __ldg(&idx[e]) >> 8;
         if (e > 0 && (__ldg(&idx[e - 1]) >> 8) == tile) continue;
         if (tile < 0 || tile >= ntiles) continue;
+        /* the run: lanes holding entries e + lane of the same tile */
+        const int code = e + lane < num ? __ldg(&idx[e + lane]) : -1;
+        const unsigned other = __ballot_sync(0xffffffffu, e + lane >= num || (code >> 8) != tile);
+        const int len = other ? __ffs(other) - 1 : 32;
+        const int pl = lane < len ? (code & 0xff) : 255;
+        bool simple = len < 32 || e + 32 >= num || (__ldg(&idx[e + 32]) >> 8) != tile;
+        int where[6];
+#pragma unroll
+        for (int pp = 0; pp < 6; pp++) {
+            const unsigned m = __ballot_sync(0xffffffffu, pl == pp);
+            where[pp] = m ? __ffs(m) - 1 : -1;
+            simple = simple && __popc(m) <= 1;
+        }
+        float *row = feat + (size_t)tile * feat_stride;
+        if (simple) {
+            float v[6][kPer];
+            float mx = 0.0f;
+#pragma unroll
+            for (int pp = 0; pp < 6; pp++) {
+                const float *src = corrs + (size_t)(e + (where[pp] < 0 ? 0 : where[pp])) * corr_stride;
+#pragma unroll
+                for (int i = 0; i < kPer; i++) {
+                    const int k = lane + 32 * i;
+                    v[pp][i] = (where[pp] >= 0 && k < n2) ? __ldg(&src[k]) : 0.0f;
+                    mx = fmaxf(mx, fabsf(v[pp][i]));
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            const float sc = mx > 0.0f ? 1.0f / mx : 0.0f;
+#pragma unroll
+            for (int pp = 0; pp < 6; pp++)
+#pragma unroll
+                for (int i = 0; i < kPer; i++) {
+                    const int k = lane + 32 * i;
+                    if (k < n2) row[pp * n2 + k] = v[pp][i] * sc;
+                }
+            continue;
+        }
         long long end = e;
         float mx = 0.0f;
         while (end < num && (__ldg(&idx[end]) >> 8) == tile) {
@@ -54,7 +98,6 @@ __global__ void __launch_bounds__(256) k_mlp_features(int ntiles, const float *_
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         const float sc = mx > 0.0f ? 1.0f / mx : 0.0f;
-        float *row = feat + (size_t)tile * feat_stride;
         for (int k = lane; k < 6 * n2; k += 32) row[k] = 0.0f;
         __syncwarp();
         for (long long e2 = e; e2 < end; e2++) {
