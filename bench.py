@@ -152,6 +152,136 @@ def barrier(pg):
         pg.barrier()
 
 
+def blob_mask(rng, tx, ty, fraction):
+    """Seeded activity mask of round blobs covering about `fraction` of the tiles."""
+    m = np.zeros((ty, tx), dtype=bool)
+    target = int(round(fraction * tx * ty))
+    yy, xx = np.mgrid[0:ty, 0:tx]
+    while m.sum() < target:
+        cy, cx = rng.integers(0, ty), rng.integers(0, tx)
+        r = rng.uniform(1.5, max(2.0, min(tx, ty) / 4))
+        m |= (yy - cy) ** 2 + (xx - cx) ** 2 <= r * r
+    return m
+
+
+class BatchedFrames:
+    """The batched workload: `n` quad frames of uneven sizes (multiples of 16
+    in 640x480 .. 2592x1936), each a crop of the full-frame scene at a seeded
+    offset with its own images, kernel table (the full table's window under
+    the crop, kernel centres moved to the crop's coordinates), and a
+    compacted task list of the tiles under seeded blobs covering 5% .. 100% of
+    the frame (tasks at the true disparity + U[-0.5, 0.5] px).  The frames run
+    one after another on one stream and share the CLT, correlation, list and
+    RGBA buffers of `pipe` (sized for the full frame)."""
+
+    def __init__(self, pipe, n=64, seed=11):
+        from tile_processor_gpu_b200 import api, synth
+        torch = pipe.torch
+        self.pipe, self.api = pipe, api
+        rng = np.random.default_rng(seed)
+        full = [h.numpy() for h in pipe.host_images]
+        gf = pipe.geom_d
+        KHf, KVf = gf["kernels_hor"], gf["kernels_vert"]
+        d0, gx, gy = pipe.scene_disparity
+        dev = pipe.images[0].device
+        self.frames = []
+        for _ in range(n):
+            w = 16 * int(rng.integers(40, WIDTH // 16 + 1))
+            h = 16 * int(rng.integers(30, HEIGHT // 16 + 1))
+            ox = 16 * int(rng.integers(0, (WIDTH - w) // 16 + 1))
+            oy = 16 * int(rng.integers(0, (HEIGHT - h) // 16 + 1))
+            geom = synth.geometry(w, h, image_rows=h + 16)
+            TX, TY, TYA = synth.tiles(geom)
+            mask = blob_mask(rng, TX, TY, float(rng.uniform(0.05, 1.0)))
+            tasks_np = synth.tasks_grid(geom, rng, jitter=0.0, disparity=(d0 + gx * ox + gy * oy, gx, gy),
+                                        mask=mask, disparity_error=DISPARITY_ERROR)
+            idx = synth.corr_indices_fast(tasks_np, geom)
+            dstride = w + 64
+            images = []
+            for c in range(4):
+                x = np.zeros((h + 16, dstride), np.float32)
+                x[:, :w] = full[c][oy:oy + h + 16, ox:ox + w]
+                images.append(torch.from_numpy(x).to(dev))
+            kh, kv, kx0, ky0 = geom["kernels_hor"], geom["kernels_vert"], ox // 16, oy // 16
+            kernels, extras = [], []
+            for c in range(4):
+                kf = pipe.kernels[c].view(KVf, KHf, 3 * 256)
+                kernels.append(kf[ky0:ky0 + kv, kx0:kx0 + kh].contiguous().view(-1))
+                ef = pipe.extra[c].view(KVf, KHf, 3, 8)[ky0:ky0 + kv, kx0:kx0 + kh].clone()
+                ef[..., 2] -= ox
+                ef[..., 3] -= oy
+                extras.append(ef.contiguous().view(-1))
+            self.frames.append(dict(
+                g=api.Geometry.from_dict(geom), TX=TX, TY=TY, dstride=dstride, size=(w, h),
+                num_tiles=int(tasks_np.size), num_corr=int(idx.size), tasks=api.tasks_to_device(tasks_np, dev),
+                corr_idx=torch.from_numpy(idx).to(dev), images=images, kernels=kernels, extras=extras,
+                p_images=api.PointerArray(images), p_kernels=api.PointerArray(kernels),
+                p_extra=api.PointerArray(extras), rgba_stride=(TX + 1) * 8))
+        self.tiles = sum(f["num_tiles"] for f in self.frames)
+        self.pixels = sum(f["size"][0] * f["size"][1] for f in self.frames)
+
+    def run_frame(self, f):
+        p, api, t = self.pipe, self.api, TEXTURE
+        api.convert_correct_tiles(f["g"], f["p_extra"], f["p_kernels"], f["p_images"], f["tasks"], p.p_clt,
+                                  f["dstride"], f["num_tiles"], 0)
+        api.correlate2D(f["g"], p.p_clt, 3, 0.25, 0.25, 0.5, FAT_ZERO, f["num_corr"], f["corr_idx"], p.corr_stride,
+                        CORR_RADIUS, p.corrs)
+        api.generate_RBGA(f["g"], f["tasks"], f["num_tiles"], p.tex_indices, p.num_tex, p.woi, f["TX"], f["TY"],
+                          p.p_clt, p.port_offsets, t["colors"], t["is_lwir"], t["min_shot"], t["scale_shot"],
+                          t["diff_sigma"], t["diff_threshold"], t["min_agree"], t["weight0"], t["weight1"],
+                          t["weight2"], t["dust_remove"], 0, f["rgba_stride"], p.rgba)
+
+    def run_all(self):
+        for f in self.frames:
+            self.run_frame(f)
+
+    def measure(self, stream, replays=10):
+        """Per-frame device time of an eager pass (CUDA events around each
+        frame's three calls) and the whole batch replayed from one CUDA graph."""
+        torch = self.pipe.torch
+        self.run_all()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in self.frames]
+        for f, (a, b) in zip(self.frames, evs):
+            a.record(stream)
+            self.run_frame(f)
+            b.record(stream)
+        torch.cuda.synchronize()
+        lat = np.array([a.elapsed_time(b) for a, b in evs])
+        eager_ms = float(lat.sum())
+        side = torch.cuda.Stream()
+        side.wait_stream(stream)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(graph, stream=side):
+                self.run_all()
+        stream.wait_stream(side)
+        graph.replay()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(replays):
+            graph.replay()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        graph_ms = g0.elapsed_time(g1) / replays
+        del graph
+        n = len(self.frames)
+        return {"frames": n, "sizes": "%dx%d .. %dx%d" % (min(f["size"][0] for f in self.frames),
+                                                         min(f["size"][1] for f in self.frames),
+                                                         max(f["size"][0] for f in self.frames),
+                                                         max(f["size"][1] for f in self.frames)),
+                "activity": "tiles under seeded blobs, 5-100% of each frame",
+                "tasks": self.tiles, "megapixels": round(self.pixels / 1e6, 1),
+                "graph_ms_per_batch": round(graph_ms, 3), "frames_per_s": round(n / graph_ms * 1e3, 1),
+                "tiles_per_s": round(self.tiles / graph_ms * 1e3, 0),
+                "eager_ms_per_batch": round(eager_ms, 3),
+                "frame_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
+                             "p99": round(float(np.percentile(lat, 99)), 4),
+                             "max": round(float(lat.max()), 4)},
+                "full_frame_equivalent_per_s": round(self.tiles / (self.pipe.TX * self.pipe.TY) / graph_ms * 1e3, 1)}
+
+
 # --------------------------------------------------------------------------- #
 # the B200 pipeline
 # --------------------------------------------------------------------------- #
@@ -167,6 +297,7 @@ class FramePipeline:
         g = self.g = api.Geometry.from_dict(self.geom_d)
         self.TX, self.TY, self.TYA = synth.tiles(self.geom_d)
         imgs, disp = synth.plane_scene(rng, WIDTH, HEIGHT, disparity=(0.0, 64.0), texture="detail")
+        self.scene_disparity = disp
         self.dstride = WIDTH + 64
         pitched = np.zeros((4, HEIGHT + 16, self.dstride), np.float32)
         pitched[:, :HEIGHT, :WIDTH] = imgs
@@ -276,10 +407,16 @@ class FramePipeline:
         torch = self.torch
         path = os.path.join(ROOT, "tile_processor_gpu_b200", "data", "disparity_mlp.npz")
         self.net = D.DisparityMLP.load(path, device=self.corrs.device)
+        try:
+            with open(os.path.splitext(path)[0] + ".json") as fh:
+                self.net_report = json.load(fh)
+        except (OSError, ValueError):
+            self.net_report = {}
         self.net.pack()
         # rows of 1352 floats start on 16-byte boundaries: 16-byte feature copies in the inference
         self.feat = torch.zeros((self.TX * self.TY, LEARNED_LDX), dtype=torch.float32, device=self.corrs.device)
         self.net_out = torch.zeros((self.TX * self.TY, 2), dtype=torch.float32, device=self.corrs.device)
+        self.learned = torch.zeros(self.TX * self.TY, dtype=torch.float32, device=self.corrs.device)
 
     def learned_features(self):
         from tile_processor_gpu_b200 import disparity_net as D
@@ -287,7 +424,9 @@ class FramePipeline:
                    feature_stride=LEARNED_LDX)
 
     def learned_infer(self):
+        """the network's {d, s} per tile and the estimate with the plain fit as fallback"""
         self.net.infer_tc(self.feat, self.TX * self.TY, self.net_out, ldx=LEARNED_LDX)
+        self.net.combine(self.disparity, self.net_out, self.TX * self.TY, self.learned)
 
     def disparity_accuracy(self):
         """RMS error of the fitted residual against the truth on tiles whose
@@ -300,12 +439,21 @@ class FramePipeline:
         res = got[inner] - self.true_residual[inner]
         learned = None
         if hasattr(self, "net_out"):
-            lg = got + self.net_out.cpu().numpy()[ty * self.TX + tx, 0].astype(np.float64)
+            tile = ty * self.TX + tx
+            lg = self.learned.cpu().numpy()[tile].astype(np.float64)
             lr = lg[inner] - self.true_residual[inner]
+            lu = (got + self.net_out.cpu().numpy()[tile, 0].astype(np.float64))[inner] - self.true_residual[inner]
+            kept = float(np.mean(self.net_out.cpu().numpy()[tile, 1][inner] < self.net.gate))
             learned = {"rmse_px": round(float(np.sqrt(np.mean(lr ** 2))), 4),
                        "outliers_gt_0.5px": round(float(np.mean(np.abs(lr) > 0.5)), 5),
-                       "net": "1350-256-128-2 GELU MLP on the six planes, shipped weights (4.87M synthetic "
-                              "tiles, 8 lenses), layer 1 TF32 and layer 2 BF16 tcgen05 MMAs (tp_mlp_infer_tc)"}
+                       "gate_logvar": self.net.gate if np.isfinite(self.net.gate) else None,
+                       "corrected_fraction": round(kept, 4),
+                       "ungated": {"rmse_px": round(float(np.sqrt(np.mean(lu ** 2))), 4),
+                                   "outliers_gt_0.5px": round(float(np.mean(np.abs(lu) > 0.5)), 5)},
+                       "net": "1350-256-128-2 GELU MLP on the six planes, shipped weights (%s synthetic tiles, "
+                              "8 lenses, planes and occlusion edges), layer 1 TF32 and layer 2 BF16 tcgen05 MMAs "
+                              "(tp_mlp_infer_tc), plain fit kept where the log-variance is above the gate "
+                              "(tp_mlp_combine)" % self.net_report.get("train_tiles", "?")}
         return {"rmse_px": round(float(np.sqrt(np.mean(res ** 2))), 4),
                 "outliers_gt_0.5px": round(float(np.mean(np.abs(res) > 0.5)), 5),
                 "truth_rms_px": round(float(np.sqrt(np.mean(self.true_residual[inner] ** 2))), 4),
@@ -349,6 +497,20 @@ def run_b200(args, rank, world, local, pg):
     build.build()
     pipe = FramePipeline(seed=100 + rank, device=dev)
     stream = torch.cuda.current_stream()
+    # launch shapes (grid caps) of the three stage kernels, tuned on this frame
+    from tile_processor_gpu_b200 import autotune
+    pipe.step()
+    torch.cuda.synchronize()
+    shapes = None
+    if args.shapes:
+        # fixed grid caps, e.g. convert=8,correlate=6,textures=4 (no tuning launches)
+        for item in args.shapes.split(","):
+            k, v = item.split("=")
+            autotune.set_shape(k.strip(), int(v))
+    elif not args.no_tune:
+        shapes = autotune.tune_stages({"convert": pipe.convert, "correlate": pipe.correlate,
+                                       "textures": pipe.texture})
+    frame_shapes = {k: autotune.get_shape(k) for k in autotune.KERNELS}
     for _ in range(args.warmup):
         pipe.step()
     torch.cuda.synchronize()
@@ -453,6 +615,20 @@ def run_b200(args, rank, world, local, pg):
         disparity["learned"]["infer_tflops"] = round(rows * 2 * (1350 * 256 + 256 * 128 + 128 * 2) / infer_ms / 1e9, 1)
         disparity["learned"]["infer_feature_gbs"] = round(rows * 1350 * 4 / infer_ms / 1e6, 1)
 
+    # ---- the batched workload: 64 uneven sparse frames, one CUDA graph ----
+    batched = None
+    if not args.no_batched:
+        batch = BatchedFrames(pipe, n=64, seed=11 + rank)
+        batch_shapes = None
+        if not args.no_tune and not args.shapes:
+            batch.run_all()
+            batch_shapes = autotune.tune_stages({"convert": batch.run_all, "correlate": batch.run_all,
+                                                 "textures": batch.run_all}, repeats=3, warmup=1)
+        batched = batch.measure(stream)
+        batched["launch_shapes"] = batch_shapes or {k: autotune.get_shape(k) for k in autotune.KERNELS}
+        for k, v in frame_shapes.items():
+            autotune.set_shape(k, v)
+
     # ---- end to end through the public API with host buffers ----
     # Every frame: its four images from pinned host memory to the device, the
     # three calls, its correlation tiles and RGBA image back to pinned host
@@ -521,6 +697,8 @@ def run_b200(args, rank, world, local, pg):
         "fused_frame_ms": round(fused_ms, 4),
         "graph_frame_ms": graph_ms,
         "disparity": disparity,
+        "batched": batched,
+        "launch_shapes": shapes or frame_shapes,
         "roofline": {"bound": "hbm", "kernel": "k_textures (%s stage)" % dom, "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
                      "algorithmic_bytes": int(algo[dom]), "traffic": int(TRAFFIC[dom]) if dom in TRAFFIC else None,
@@ -618,6 +796,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample-tiles", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-frame batched workload")
+    ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes instead of tuned ones")
+    ap.add_argument("--shapes", default="", help="fixed launch shapes, e.g. convert=8,correlate=6,textures=4")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU arm: rank 0 alone runs it, the other ranks exit without work

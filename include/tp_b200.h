@@ -124,6 +124,26 @@ int tp_get_lpf(int which, float *values);
 /* Restore the built-in tables on the current device. */
 int tp_reset_lpf(void);
 
+/* ---- launch shapes ----------------------------------------------------------
+ * No counterpart in the reference (its launches are fixed).  The stage kernels
+ * walk their work items with grid-stride loops over a grid capped at
+ * ctas_per_sm x the SM count; the cap sets how many tiles each CTA takes in
+ * turn.  0 restores the built-in value (convert 8, correlate 6, textures 4).
+ * Process-wide, read at every launch (a CUDA graph keeps the shape it was
+ * captured with).  tile_processor_gpu_b200.autotune picks the value by timing
+ * the caller's workload. */
+enum {
+    TP_SHAPE_CONVERT = 0,   /* k_convert_correct_tiles (tp_convert_correct_tiles) */
+    TP_SHAPE_CORRELATE = 1, /* k_correlate2D (tp_correlate2D)                     */
+    TP_SHAPE_TEXTURES = 2,  /* k_textures (tp_textures_accumulate, generate_RBGA) */
+    TP_SHAPE_COUNT = 3
+};
+#define TP_MAX_CTAS_PER_SM 32
+/* TP_ERR_ARG for an unknown kernel or a value outside 0..TP_MAX_CTAS_PER_SM */
+int tp_set_launch_shape(int kernel, int ctas_per_sm);
+/* the value in use (the built-in one when unset), TP_ERR_ARG for an unknown kernel */
+int tp_get_launch_shape(int kernel);
+
 /* ---- forward CLT with aberration correction ---------------------------------
  * Replaces convert_correct_tiles (src/TileProcessor.cuh:1859-1937).
  * kernel_offsets : device array [4] of device tp_clt_extra[kv*kh*3]
@@ -395,6 +415,11 @@ int tp_mlp_nll(int rows, const float *out, const float *target, const float *w, 
 int tp_mlp_pack(const float *W1, const float *W2, void *w1t, void *w2t, tp_stream_t stream);
 int tp_mlp_infer_tc(int rows, const float *x, int ldx, const void *w1t, const float *b1, const void *w2t,
                     const float *b2, const float *W3, const float *b3, float *out, int *err, tp_stream_t stream);
+/* The learned estimate with the plain fit as its fallback: rho[i] = plain[i]
+ * + out[i].d where out[i].s (the log-variance) < gate, else plain[i]; out is
+ * the {d, s} pairs of tp_mlp_infer_tc (8-byte aligned).  gate = +inf keeps
+ * every correction. */
+int tp_mlp_combine(size_t n, const float *plain, const float *out, float gate, float *rho, tp_stream_t stream);
 /* Adam step `step` (1, 2, ...) on n parameters */
 int tp_mlp_adam(size_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1, float beta2,
                 float eps, int step, tp_stream_t stream);

@@ -104,6 +104,36 @@ def test_plane_scene_accuracy(oracle):
     assert np.polyfit(truth[inner], got[inner], 1)[0] > 0.6
 
 
+def test_occlusion_scene_geometry(oracle):
+    """Two planes with an occlusion edge (the learned residual's training
+    scenes): tasks placed by the per-point disparity function, one pass of
+    the plain method, noise-free.  Tiles whose footprint stays on one side
+    of the edge match the truth as on a single plane; tiles straddling the
+    edge are worse."""
+    W = H = 256
+    rng = np.random.default_rng(21)
+    g = S.geometry(W, H, image_rows=H + 16)
+    imgs, dfun = S.occlusion_scene(rng, W, H, disparity=(0.0, 24.0), gain=0.0, read_sigma=0.0)
+    pit = S.pitched(imgs, W + 64, H + 16)
+    kern, extra = S.kernel_tables(rng, g, pool=64, zero_extra=True, psf_offset=0.0)
+    tasks, e = S.tasks_grid(g, rng, jitter=0.0, disparity=dfun, disparity_error=0.5, return_error=True)
+    clt = oracle.convert_correct_tiles(g, extra, kern, pit, W + 64, tasks)
+    idx = S.corr_indices_fast(tasks, g)
+    co = oracle.correlate2D(g, clt, 3, .25, .25, .5, 0.05, idx, 225, 7)
+    d, _ = oracle.disparity_fit(g, co, idx, 7, mode=0)
+    TX, TY = W // 8, H // 8
+    tx, ty = tasks["txy"] & 0xFFFF, tasks["txy"] >> 16
+    res = d[ty * TX + tx] + e
+    nx, ny, c = dfun.edge
+    dist = np.abs(nx * (tx * 8 + 4) + ny * (ty * 8 + 4) - c)
+    inner = (tx >= 3) & (tx < TX - 3) & (ty >= 3) & (ty < TY - 3)
+    far, near = inner & (dist > 24), inner & (dist < 6)
+    assert far.sum() > 100 and near.sum() > 10
+    rms_far, rms_near = np.sqrt(np.mean(res[far] ** 2)), np.sqrt(np.mean(res[near] ** 2))
+    assert rms_far < 0.2, rms_far
+    assert rms_near > rms_far
+
+
 def test_plane_scene_noise_free(oracle):
     """Without noise one pass is within 0.2 px RMS."""
     got, truth, inner = _plane_pipeline(oracle, 256, 256, 0.5, 8, noise=False)

@@ -41,3 +41,38 @@ def test_loss_of_a_known_case(oracle):
     loss, _ = oracle.mlp_loss_and_grads(p, x, t)
     want = np.mean(0.5 * np.exp(-0.5) * (0.2 - t) ** 2 + 0.25)
     assert abs(loss - want) < 1e-12
+
+
+def test_fallback_gate_choice():
+    """The validation rule of the fallback gate: corrections that help where
+    the network is confident and hurt where it is not are kept only below a
+    log-variance quantile; a network that helps everywhere keeps them all."""
+    import torch
+    from tile_processor_gpu_b200 import disparity_net as D
+    g = torch.Generator().manual_seed(3)
+    n = 20000
+    truth = torch.randn(n, generator=g) * 0.3
+    plain = truth + torch.randn(n, generator=g) * 0.2
+    logvar = torch.rand(n, generator=g) * 4 - 2
+    good = truth + torch.randn(n, generator=g) * 0.05
+    bad = truth + torch.randn(n, generator=g) * 0.8
+    rho = torch.where(logvar < 1.0, good, bad)           # the top quarter of logvar is harmful
+    gate, table = D.choose_gate(rho, logvar, plain, truth)
+    assert 0.5 < gate <= 1.2, gate
+    assert D.accuracy(D.gated(rho, logvar, plain, gate), truth)["rmse_px"] < D.accuracy(rho, truth)["rmse_px"]
+    gate2, _ = D.choose_gate(good, logvar, plain, truth)
+    assert gate2 == float("inf")
+
+
+def test_gate_saved_with_the_weights(tmp_path):
+    from tile_processor_gpu_b200 import disparity_net as D
+    net = D.DisparityMLP(device="cpu", seed=4)
+    net.gate = 0.75
+    net.save(str(tmp_path / "n.npz"))
+    back = D.DisparityMLP.load(str(tmp_path / "n.npz"), device="cpu")
+    assert back.gate == 0.75
+    assert all(np.array_equal(back.p[k].numpy(), np.float16(net.p[k].numpy()).astype(np.float32) if k.startswith("W")
+                              else net.p[k].numpy()) for k in D.PARAMS)
+    net.gate = float("inf")
+    net.save(str(tmp_path / "m.npz"))
+    assert D.DisparityMLP.load(str(tmp_path / "m.npz"), device="cpu").gate == float("inf")

@@ -145,6 +145,24 @@ def test_features_irregular_runs(native):
     assert np.all(got[untouched] == -5.0)
 
 
+def test_combine_with_fallback(native):
+    """tp_mlp_combine: plain + d where s < gate, plain elsewhere; +inf keeps all."""
+    import torch
+    from tile_processor_gpu_b200 import disparity_net as D
+    rng = np.random.default_rng(8)
+    n = 100003
+    plain = rng.normal(0, 1, n).astype(np.float32)
+    out = rng.normal(0, 1, (n, 2)).astype(np.float32)
+    net = D.DisparityMLP(seed=0)
+    rho = torch.full((n,), -7.0, device="cuda")
+    for gate in (0.25, float("inf"), -10.0):
+        net.gate = gate
+        net.combine(_dev(plain), _dev(out), n, rho)
+        torch.cuda.synchronize()
+        want = plain + np.where(out[:, 1] < gate, out[:, 0], 0.0).astype(np.float32)
+        assert np.array_equal(rho.cpu().numpy(), want)
+
+
 def test_learned_residual_beats_plain_fit(native):
     """Trained on eight synthetic frames, on a held-out frame the network's
     estimate (plain fit + correction) has a smaller RMS error against the

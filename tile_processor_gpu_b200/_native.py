@@ -74,12 +74,15 @@ SIGNATURES = {
     "tp_mlp_pack": [_P, _P, _P, _P, _P],
     "tp_mlp_infer_tc": [_I, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "tp_mlp_adam": [_S, _P, _P, _P, _P, _F, _F, _F, _F, _I, _P],
+    "tp_mlp_combine": [_S, _P, _P, _F, _P, _P],
     "tp_set_lpf": [_I, _P],
     "tp_get_lpf": [_I, _P],
     "tp_reset_lpf": [],
     "tp_tiles_x": [_G],
     "tp_tiles_y": [_G],
     "tp_tiles_ya": [_G],
+    "tp_set_launch_shape": [_I, _I],
+    "tp_get_launch_shape": [_I],
 }
 STRING_FUNCS = ("tp_last_error", "tp_version")
 # entry points returning a count (long long) instead of a status

@@ -10,6 +10,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <math.h>
+#include <atomic>
 #include <mutex>
 #include <stdarg.h>
 #include <stdio.h>
@@ -97,6 +98,16 @@ unsigned grid_for(long long items, int items_per_block, int sms, int per_sm)
     return (unsigned)need;
 }
 
+/* grid caps of the stage kernels in CTAs per SM (0 = the built-in value) */
+std::atomic<int> g_shape[TP_SHAPE_COUNT];
+const int g_shape_default[TP_SHAPE_COUNT] = {8, 6, 4};
+
+int shape_per_sm(int which)
+{
+    const int v = g_shape[which].load(std::memory_order_relaxed);
+    return v > 0 ? v : g_shape_default[which];
+}
+
 /* Kernels taking more shared memory than the 48 KB granted by default get
  * their attribute once per device (the first call; make it before capturing
  * a stream into a graph). */
@@ -176,6 +187,21 @@ int tensor_map_encoder(PFN_cuTensorMapEncodeTiled_v12000 *fn)
 extern "C" {
 
 const char *tp_last_error(void) { return g_err; }
+
+int tp_set_launch_shape(int kernel, int ctas_per_sm)
+{
+    if (kernel < 0 || kernel >= TP_SHAPE_COUNT) return fail(TP_ERR_ARG, "launch shape kernel %d", kernel);
+    if (ctas_per_sm < 0 || ctas_per_sm > TP_MAX_CTAS_PER_SM)
+        return fail(TP_ERR_ARG, "ctas_per_sm %d outside 0..%d", ctas_per_sm, TP_MAX_CTAS_PER_SM);
+    g_shape[kernel].store(ctas_per_sm, std::memory_order_relaxed);
+    return TP_OK;
+}
+
+int tp_get_launch_shape(int kernel)
+{
+    if (kernel < 0 || kernel >= TP_SHAPE_COUNT) return fail(TP_ERR_ARG, "launch shape kernel %d", kernel);
+    return shape_per_sm(kernel);
+}
 const char *tp_version(void) { return TP_VERSION; }
 
 int tp_tiles_x(const tp_geometry *g) { return g ? g->img_width / 8 : 0; }
@@ -223,7 +249,7 @@ int tp_convert_correct_tiles(const tp_geometry *g, float *const *kernel_offsets,
     int sms;
     if ((rc = sm_count(&sms))) return rc;
     const long long warps = (long long)((num_tiles + 3) / 4) * 12;
-    unsigned grid = grid_for(warps, 8, sms, 8);
+    unsigned grid = grid_for(warps, 8, sms, shape_per_sm(TP_SHAPE_CONVERT));
     tp::k_convert_correct_tiles<<<grid, 256, 0, (cudaStream_t)stream>>>(
         gd, dstride, kernel_offsets, kernels, images, tasks, clt, num_tiles, lpf_mask);
     return cuda_status(cudaGetLastError(), "convert_correct_tiles launch");
@@ -246,7 +272,7 @@ int tp_correlate2D(const tp_geometry *g, float *const *clt, int colors, float sc
     if (corr_stride < sz) return fail(TP_ERR_ARG, "corr_stride %zu < (2r+1)^2 = %zu", corr_stride, sz);
     int sms;
     if ((rc = sm_count(&sms))) return rc;
-    unsigned grid = grid_for((long long)num_corr_tiles, 16, sms, 6);
+    unsigned grid = grid_for((long long)num_corr_tiles, 16, sms, shape_per_sm(TP_SHAPE_CORRELATE));
     tp::k_correlate2D<<<grid, 128, 0, (cudaStream_t)stream>>>(gd, clt, colors, scale0, scale1, scale2, fat_zero,
                                                               (long long)num_corr_tiles, corr_indices,
                                                               corr_stride, corr_radius, corrs);
@@ -298,7 +324,7 @@ int tp_textures_accumulate(const tp_geometry *g, const int *woi, float *const *c
     int sms;
     if ((rc = sm_count(&sms))) return rc;
     if ((rc = texture_smem_setup())) return rc;
-    unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, 4);
+    unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
     tp::k_textures<<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
         gd, woi, clt, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
@@ -413,7 +439,7 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
                                                                          texture_tiles);
     }
     const int quarter = gd.TX * (gd.TYA >> 2);
-    const unsigned grid = grid_for(quarter, 1, sms, 4);
+    const unsigned grid = grid_for(quarter, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
     if ((rc = texture_smem_setup())) return rc;
     for (int pass = 0; pass < 8; pass++) {
         const int border = pass >> 2;
@@ -619,6 +645,18 @@ int tp_mlp_infer_tc(int rows, const float *x, int ldx, const void *w1t, const fl
         tmap, rows, static_cast<const float *>(w1t), b1, static_cast<const __nv_bfloat16 *>(w2t), b2, W3, b3, out,
         err);
     return cuda_status(cudaGetLastError(), "mlp_infer_tc launch");
+}
+
+int tp_mlp_combine(size_t n, const float *plain, const float *out, float gate, float *rho, tp_stream_t stream)
+{
+    if (!n) return TP_OK;
+    if (!plain || !out || !rho) return fail(TP_ERR_ARG, "NULL mlp_combine operand");
+    if (reinterpret_cast<uintptr_t>(out) & 7) return fail(TP_ERR_ARG, "out must be 8-byte aligned");
+    int sms, rc;
+    if ((rc = sm_count(&sms))) return rc;
+    tp::k_mlp_combine<<<grid_for((long long)n, 256, sms, 8), 256, 0, (cudaStream_t)stream>>>((long long)n, plain, out,
+                                                                                          gate, rho);
+    return cuda_status(cudaGetLastError(), "mlp_combine launch");
 }
 
 int tp_mlp_adam(size_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1, float beta2,

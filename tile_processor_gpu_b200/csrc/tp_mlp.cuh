@@ -108,6 +108,19 @@ __global__ void __launch_bounds__(256) k_mlp_features(int ntiles, const float *_
     }
 }
 
+/* ---- the learned estimate with the plain fit as fallback -------------------
+ * rho[i] = plain[i] + d_i where the network's log-variance s_i < gate, else
+ * plain[i] (out[i] = {d_i, s_i}). */
+__global__ void __launch_bounds__(256) k_mlp_combine(long long n, const float *__restrict__ plain,
+                                                     const float *__restrict__ out, float gate,
+                                                     float *__restrict__ rho)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float2 o = reinterpret_cast<const float2 *>(out)[i];
+        rho[i] = plain[i] + (o.y < gate ? o.x : 0.0f);
+    }
+}
+
 /* ---- GEMM ----------------------------------------------------------------- */
 
 /* C[M][N] = beta C + op(A) op(B) (+ bias[n]); op(A) is M x K (A[m][k], or

@@ -166,14 +166,27 @@ class DisparityMLP:
     def host_params(self):
         return {k: v.cpu().numpy().copy() for k, v in self.p.items()}
 
+    # log-variance above which the plain fit is kept (combine); +inf keeps every correction
+    gate = float("inf")
+
+    def combine(self, plain, out, rows, rho, stream=None):
+        """rho = plain + d where the log-variance s < self.gate, else plain (tp_mlp_combine)."""
+        _native.call("tp_mlp_combine", int(rows), _dptr(plain), _dptr(out), float(self.gate), _dptr(rho),
+                     _stream(stream))
+        return rho
+
     def save(self, path):
-        np.savez_compressed(path, **{k: v.astype(np.float16 if k.startswith("W") else np.float32)
-                                     for k, v in self.host_params().items()})
+        arrays = {k: v.astype(np.float16 if k.startswith("W") else np.float32) for k, v in self.host_params().items()}
+        arrays["gate"] = np.array(self.gate, np.float32)
+        np.savez_compressed(path, **arrays)
 
     @classmethod
     def load(cls, path, device="cuda"):
         d = np.load(path)
-        return cls({k: d[k].astype(np.float32) for k in PARAMS}, device=device)
+        net = cls({k: d[k].astype(np.float32) for k in PARAMS}, device=device)
+        if "gate" in d.files:
+            net.gate = float(d["gate"])
+        return net
 
 
 # --------------------------------------------------------------------------- #
@@ -242,6 +255,29 @@ def train(net, feats, plain, truth, epochs=4, batch=4096, lr=1e-3, seed=0, log=N
         if log is not None:
             log(ep, total / max(nb, 1))
     return net
+
+
+def gated(rho, logvar, plain, gate):
+    """The estimate with the plain fit kept where logvar >= gate (evaluation
+    helper on device tensors; tp_mlp_combine is the library form)."""
+    torch = _t()
+    return torch.where(logvar < gate, rho, plain)
+
+
+def choose_gate(rho, logvar, plain, truth, quantiles=(0.5, 0.6, 0.7, 0.8, 0.85, 0.9, 0.95, 0.98, 0.99)):
+    """Pick the log-variance gate on validation samples: among +inf and the
+    given quantiles of logvar, the one with the fewest > 0.5 px errors whose
+    RMS error stays within 0.5% of the best RMS error.  Returns (gate, table)."""
+    torch = _t()
+    cands = [float("inf")] + [float(torch.quantile(logvar.float().cpu(), q)) for q in quantiles]
+    table = []
+    for g in cands:
+        a = accuracy(gated(rho, logvar, plain, g), truth)
+        table.append((g, a["rmse_px"], a["outliers_gt_0.5px"]))
+    best_rmse = min(t[1] for t in table)
+    ok = [t for t in table if t[1] <= best_rmse * 1.005]
+    gate = min(ok, key=lambda t: (t[2], t[1]))[0]
+    return gate, table
 
 
 def predict(net, feats, plain, batch=16384):

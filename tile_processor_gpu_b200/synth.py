@@ -126,6 +126,80 @@ def plane_scene(rng, width, height, disparity=(0.0, 64.0), port_offsets=PORT_OFF
     return np.stack(imgs), (d0, gx, gy)
 
 
+class TwoPlaneDisparity:
+    """d(x, y) of occlusion_scene: the foreground plane where n . (x, y) > c,
+    else the background plane (a picklable callable)."""
+
+    def __init__(self, back, front, edge):
+        self.back, self.front, self.edge = tuple(back), tuple(front), tuple(edge)
+
+    def __call__(self, x, y):
+        x = np.asarray(x, np.float64); y = np.asarray(y, np.float64)
+        (b0, bx, by), (f0, fx, fy), (nx, ny, c) = self.back, self.front, self.edge
+        return np.where(nx * x + ny * y > c, f0 + fx * x + fy * y, b0 + bx * x + by * y)
+
+
+def occlusion_scene(rng, width, height, disparity=(0.0, 64.0), port_offsets=PORT_OFFSETS, gain=0.01,
+                    read_sigma=0.002, peak=1.0, texture="detail"):
+    """Quad-camera Bayer frame of two slanted textured planes with an
+    occlusion edge.
+
+    The background plane B spans the lower part of `disparity`; the
+    foreground plane F = B + delta (delta 4..16 px, its own small slope) is
+    nearer everywhere and covers the scene points s with n . s > c, a seeded
+    straight edge through the frame.  Camera k shows at pixel p the
+    foreground point s_F (the inverse of p = s + d_F(s) o_k, as in
+    plane_scene) when s_F lies in the foreground region, else the background
+    point s_B; the two planes carry independent textures.  Returns (images,
+    d) with d(x, y) the disparity of the surface seen at scene point (x, y)
+    in the reference view (F inside the region, B outside)."""
+    H, W = height, width
+    scales, weights = TEXTURES[texture]
+    texb = np.stack([smooth_noise(rng, H + 96, W + 96, scales=scales, weights=weights) for _ in range(3)])
+    texf = np.stack([smooth_noise(rng, H + 96, W + 96, scales=scales, weights=weights) for _ in range(3)])
+    dlo, dhi = disparity
+    delta = rng.uniform(4.0, 16.0)
+    span = max(dhi - dlo - delta - 4.0, 1.0)
+    gxb = span * rng.uniform(0.3, 0.7) / W
+    gyb = (span - gxb * W) / H
+    d0b = dlo
+    gxf = gxb + rng.uniform(-2.0, 2.0) / W
+    gyf = gyb + rng.uniform(-2.0, 2.0) / H
+    d0f = d0b + delta + 2.0
+    ang = rng.uniform(0, 2 * math.pi)
+    nx, ny = math.cos(ang), math.sin(ang)
+    px, py = rng.uniform(0.3, 0.7) * W, rng.uniform(0.3, 0.7) * H
+    cc = nx * px + ny * py
+
+    dfun = TwoPlaneDisparity((d0b, gxb, gyb), (d0f, gxf, gyf), (nx, ny, cc))
+
+    cmap = bayer_color_map(H, W)
+    yy, xx = np.mgrid[0:H, 0:W].astype(np.float64)
+
+    def inverse(k, d0, gx, gy):
+        ox, oy = float(port_offsets[k][0]), float(port_offsets[k][1])
+        qx, qy = xx - d0 * ox, yy - d0 * oy
+        gq = (gx * qx + gy * qy) / (1.0 + gx * ox + gy * oy)
+        return qx - ox * gq, qy - oy * gq
+
+    def sample(tex, sx, sy):
+        sx = sx + 48.0; sy = sy + 48.0
+        x0 = np.clip(np.floor(sx).astype(np.int64), 0, W + 94); fx = sx - x0
+        y0 = np.clip(np.floor(sy).astype(np.int64), 0, H + 94); fy = sy - y0
+        return tex[cmap, y0, x0] * (1 - fx) * (1 - fy) + tex[cmap, y0, x0 + 1] * fx * (1 - fy) + \
+            tex[cmap, y0 + 1, x0] * (1 - fx) * fy + tex[cmap, y0 + 1, x0 + 1] * fx * fy
+
+    imgs = []
+    for k in range(len(port_offsets)):
+        fxs, fys = inverse(k, d0f, gxf, gyf)
+        bxs, bys = inverse(k, d0b, gxb, gyb)
+        fg = nx * fxs + ny * fys > cc
+        v = peak * np.where(fg, sample(texf, fxs, fys), sample(texb, bxs, bys))
+        v = v + np.sqrt(np.maximum(gain * v, 0.0)) * rng.standard_normal(v.shape) + read_sigma * rng.standard_normal(v.shape)
+        imgs.append(v.astype(np.float32))
+    return np.stack(imgs), dfun
+
+
 def pitched(images, dstride, rows=None, fill=0.0):
     """Copy [cams][H][W] into [cams][rows][dstride] (extra rows / columns = fill)."""
     cams, H, W = images.shape
@@ -204,7 +278,8 @@ def tasks_grid(geom, rng=None, jitter=0.5, task_bits=ALL_TASK_BITS, disparity=No
 
     xy[cam] = tile centre (8 tx + 4, 8 ty + 4) + U[-jitter, jitter] per
     camera + (d(tx, ty) + e) * port_offsets[cam] when `disparity` = (d0, gx,
-    gy), rounded to 1/256 px; e = U[-disparity_error, disparity_error] per
+    gy) (d = d0 + gx x + gy y at the tile centre) or a function d(x, y),
+    rounded to 1/256 px; e = U[-disparity_error, disparity_error] per
     tile, the same for all cameras (the task's disparity error, so the tile's
     residual disparity is -e).  With return_error, returns (tasks, e)."""
     TX, TY, _ = tiles(geom)
@@ -228,8 +303,11 @@ def tasks_grid(geom, rng=None, jitter=0.5, task_bits=ALL_TASK_BITS, disparity=No
             x += rng.uniform(-jitter, jitter, n)
             y += rng.uniform(-jitter, jitter, n)
         if disparity is not None:
-            d0, gx, gy = disparity
-            d = d0 + gx * cx + gy * cy + err
+            if callable(disparity):
+                d = disparity(cx, cy) + err
+            else:
+                d0, gx, gy = disparity
+                d = d0 + gx * cx + gy * cy + err
             x += d * port_offsets[cam][0]
             y += d * port_offsets[cam][1]
         t["xy"][:, cam, 0] = np.round(x * 256.0) / 256.0

@@ -1,16 +1,20 @@
 """Train the learned disparity residual on synthetic scenes of known disparity.
 
-    python -m tile_processor_gpu_b200.train_disparity --frames 200 --holdout 8 \
+    python -m tile_processor_gpu_b200.train_disparity --frames 800 --holdout 24 \
         --out tile_processor_gpu_b200/data/disparity_mlp.npz
 
-Each frame is a seeded slanted textured plane (disparity from 0 to 8..64 px
-across the frame, shot and read noise) seen through one of eight lenses
-(kernel tables of 256 PSF shapes each), whose tiles are tasked at the true
-disparity plus a per-tile error U[-e, e] px, e drawn per frame in [0.3, 1.2].
-The library's own pipeline (forward CLT, pair correlation, plain fit,
-features) turns each frame into samples; the network
-is trained with its own kernels (disparity_net) and evaluated on held-out
-seeds against the plain fit, with both the FP32 and the tensor-core inference.
+Each frame is a seeded slanted textured plane, or (a third of the frames)
+two planes with an occlusion edge, disparity from 0 to 8..64 px across the
+frame, shot noise and a read-noise sigma drawn log-uniformly in
+[0.001, 0.02], seen through one of eight lenses (kernel tables of 256 PSF
+shapes each); its tiles are tasked at the true disparity plus a per-tile
+error U[-e, e] px, e drawn per frame in [0.3, 1.2].  The library's own
+pipeline (forward CLT, pair correlation, plain fit, features) turns each
+frame into samples; the network is trained with its own kernels
+(disparity_net).  Eight validation frames choose the log-variance gate above
+which the plain fit is kept (the fallback); held-out frames then compare the
+plain fit, the network and the gated network, overall and per scene kind,
+with both the FP32 and the tensor-core inference.
 Scene rendering runs in spawned worker processes (NumPy only).
 """
 import argparse
@@ -26,9 +30,15 @@ W_DEF, H_DEF = 1024, 768
 
 
 def _frame_draws(seed):
-    """per-frame disparity span, task error and lens index"""
+    """per-frame disparity span, task error, lens index, scene kind (a third
+    of the frames have an occlusion edge) and read-noise sigma (log-uniform)"""
     r = np.random.default_rng(seed + 7_000_001)
-    return float(r.uniform(8.0, 64.0)), float(r.uniform(0.3, 1.2)), int(r.integers(0, N_LENSES))
+    return (float(r.uniform(8.0, 64.0)), float(r.uniform(0.3, 1.2)), int(r.integers(0, N_LENSES)),
+            "occlusion" if r.uniform() < OCCLUSION_FRACTION else "plane",
+            float(np.exp(r.uniform(np.log(0.001), np.log(0.02)))))
+
+
+OCCLUSION_FRACTION = 1.0 / 3.0
 
 
 N_LENSES = 8
@@ -37,9 +47,10 @@ N_LENSES = 8
 def _render(args):
     seed, width, height = args
     from tile_processor_gpu_b200 import synth
-    span, _, _ = _frame_draws(seed)
+    span, _, _, kind, sigma = _frame_draws(seed)
     rng = np.random.default_rng(seed)
-    imgs, disp = synth.plane_scene(rng, width, height, disparity=(0.0, span), texture="detail")
+    scene = synth.occlusion_scene if kind == "occlusion" else synth.plane_scene
+    imgs, disp = scene(rng, width, height, disparity=(0.0, span), texture="detail", read_sigma=sigma)
     return seed, imgs, disp
 
 
@@ -91,23 +102,26 @@ def make_lens(width, height, seed=7, device="cuda"):
 
 
 def build_set(seeds, width, height, lenses, workers):
+    """features, plain residual, true residual and scene kind (1 = occlusion) per sample"""
     import torch
-    feats, plains, truths = [], [], []
+    feats, plains, truths, kinds = [], [], [], []
     with mp.get_context("spawn").Pool(workers) as pool:
         for seed, imgs, disp in pool.imap(_render, [(s, width, height) for s in seeds]):
-            _, err, li = _frame_draws(seed)
+            _, err, li, kind, _ = _frame_draws(seed)
             f, p, t = samples_from_scene(seed, imgs, disp, lenses[li], width, height, error=err)
             feats.append(f)
             plains.append(p)
             truths.append(t)
-    return torch.cat(feats), torch.cat(plains), torch.cat(truths)
+            kinds.append(torch.full_like(t, 1.0 if kind == "occlusion" else 0.0))
+    return torch.cat(feats), torch.cat(plains), torch.cat(truths), torch.cat(kinds)
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--frames", type=int, default=200)
-    ap.add_argument("--holdout", type=int, default=8)
-    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--frames", type=int, default=800)
+    ap.add_argument("--holdout", type=int, default=24)
+    ap.add_argument("--validation", type=int, default=8, help="frames that choose the fallback gate")
+    ap.add_argument("--epochs", type=int, default=14)
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--width", type=int, default=W_DEF)
@@ -123,24 +137,40 @@ def main(argv=None):
     lenses = [make_lens(args.width, args.height, seed=100 + i) for i in range(N_LENSES)]
     train_seeds = list(range(10_000, 10_000 + args.frames))
     hold_seeds = list(range(90_000, 90_000 + args.holdout))
-    feats, plain, truth = build_set(train_seeds, args.width, args.height, lenses, args.workers)
-    hf, hp, ht = build_set(hold_seeds, args.width, args.height, lenses, args.workers)
+    val_seeds = list(range(80_000, 80_000 + args.validation))
+    feats, plain, truth, _ = build_set(train_seeds, args.width, args.height, lenses, args.workers)
+    hf, hp, ht, hk = build_set(hold_seeds, args.width, args.height, lenses, args.workers)
+    vf, vp, vt, _ = build_set(val_seeds, args.width, args.height, lenses, args.workers)
     t1 = time.time()
     net = D.DisparityMLP(seed=1)
     log = lambda ep, loss: print("epoch %d loss %.5f" % (ep, loss), file=sys.stderr, flush=True)
     D.train(net, feats, plain, truth, epochs=args.epochs, batch=args.batch, lr=args.lr, log=log)
     torch.cuda.synchronize()
     t2 = time.time()
+    # the plain fit as fallback: a log-variance gate chosen on the validation frames
+    vrho, vlogvar = D.predict(net, vf, vp)
+    net.gate, gate_table = D.choose_gate(vrho, vlogvar, vp, vt)
+    del vf
     rho, logvar = D.predict(net, hf, hp)
+    rho_g = D.gated(rho, logvar, hp, net.gate)
     net.pack()
     out_tc = torch.empty((hf.shape[0], 2), dtype=torch.float32, device=hf.device)
     net.infer_tc(D.pad_rows(hf), hf.shape[0], out_tc)
     torch.cuda.synchronize()
+    fin = lambda v: v if np.isfinite(v) else None  # noqa: E731  (no gate: null)
     report = {"train_tiles": int(feats.shape[0]), "holdout_tiles": int(hf.shape[0]), "frames": args.frames,
               "holdout_frames": args.holdout, "epochs": args.epochs, "frame": "%dx%d" % (args.width, args.height),
               "lenses": N_LENSES, "disparity_span_px": [8, 64], "task_error_px": [0.3, 1.2],
+              "scenes": "slanted planes; a third two planes with an occlusion edge",
+              "read_sigma": "log-uniform in [0.001, 0.02]",
+              "validation_frames": args.validation, "gate_logvar": fin(net.gate),
+              "gate_table": [{"gate": fin(g), "rmse_px": r, "outliers_gt_0.5px": o} for g, r, o in gate_table],
               "plain": D.accuracy(hp, ht), "learned_fp32": D.accuracy(rho, ht),
+              "learned_gated": D.accuracy(rho_g, ht),
               "learned_tensor_core": D.accuracy(hp + out_tc[:, 0], ht),
+              "by_scene": {name: {"tiles": int(m.sum().item()), "plain": D.accuracy(hp[m], ht[m]),
+                                  "learned": D.accuracy(rho[m], ht[m]), "learned_gated": D.accuracy(rho_g[m], ht[m])}
+                           for name, m in (("plane", hk == 0), ("occlusion", hk == 1)) if int(m.sum().item())},
               "seconds": {"data": round(t1 - t0, 1), "train": round(t2 - t1, 1)}}
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     net.save(args.out)
