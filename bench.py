@@ -463,7 +463,7 @@ class FramePipeline:
                                                                                         DISPARITY_ERROR)}
 
     STAGES = ("convert", "correlate", "texture")
-    LAUNCHES = {"convert": 1, "correlate": 1, "texture": 15}
+    LAUNCHES = {"convert": 1, "correlate": 1, "texture": 11}  # texture: 6 list kernels, RGBA clear, 4 passes
     FRAME_LAUNCHES = 11  # 6 list kernels, RGBA clear, 4 parity launches
 
     def step(self):

@@ -441,13 +441,14 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
     const int quarter = gd.TX * (gd.TYA >> 2);
     const unsigned grid = grid_for(quarter, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
     if ((rc = texture_smem_setup())) return rc;
-    for (int pass = 0; pass < 8; pass++) {
-        const int border = pass >> 2;
-        const int slot = ((pass & 3) << 1) + border;
-        const int *base = texture_indices + (pass & 3) * quarter;
-        tp::k_textures<<<grid, tp::kTexThreads, tp::kTexSmemBytes, s>>>(gd, woi, clt, 0, base, num_texture_tiles, slot, quarter,
-                                            border ? quarter : 0, port_offsets, p, texture_rbga_stride,
-                                            texture_tiles, 0, nullptr);
+    /* one pass per tile parity: its inner sub-list, then its border one (the
+     * reference runs the four inner passes, then the four border passes;
+     * tiles of one parity never overlap, so a pass needs no ordering) */
+    for (int parity = 0; parity < 4; parity++) {
+        const int *base = texture_indices + parity * quarter;
+        tp::k_textures<<<grid, tp::kTexThreads, tp::kTexSmemBytes, s>>>(
+            gd, woi, clt, 0, base, num_texture_tiles, parity << 1, quarter, -quarter, port_offsets, p,
+            texture_rbga_stride, texture_tiles, 0, nullptr);
     }
     return cuda_status(cudaGetLastError(), "generate_RBGA launch");
 }

@@ -376,12 +376,29 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
 
     long long count = num_texture_tiles;
     const int *lst = list;
+    /* entries at or past `split` sit `gap` further on in the list */
+    int split = 0x7fffffff, gap = 0;
     if (dev_counts) {
         /* sub-list length from the list builder, kept inside its quarter */
         count = dev_counts[count_slot];
         count = count < 0 ? 0 : (count > list_cap ? list_cap : count);
-        if (border_quarter) lst = list + (border_quarter - count);
+        if (border_quarter > 0) {
+            /* the border sub-list alone: it grows down from the quarter's end */
+            lst = list + (border_quarter - count);
+        } else if (border_quarter < 0) {
+            /* inner (count_slot) then border (count_slot + 1) sub-lists of one
+             * quarter of -border_quarter entries in one pass: tiles of one
+             * parity never overlap, so their RGBA updates need no ordering */
+            const int q = -border_quarter, ci = (int)count;
+            int cb = dev_counts[count_slot + 1];
+            cb = cb < 0 ? 0 : (cb > q - ci ? q - ci : cb);
+            split = ci;
+            gap = q - cb - ci;
+            count += cb;
+        }
     }
+    /* list entry n of this pass */
+    auto code_at = [&](long long n) -> int { return lst[n + (n >= split ? gap : 0)]; };
     const bool want_rbg = texture_rbg && texture_rbg_stride;
     const bool want_tiles = texture_tiles && texture_stride;
     const int ns_tiles = (colors == 3) ? (p.keep_weights ? 12 : 4) : (p.keep_weights ? 8 : 2);
@@ -395,7 +412,7 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     /* list entry -> tile index, or -1 when the entry is not a texture tile */
     auto tile_of = [&](long long n) -> int {
         if (n >= count) return -1;
-        const int code = lst[n];
+        const int code = code_at(n);
         const int tile = code >> 8;
         return ((code & (1 << 7)) && tile >= 0 && tile < ntiles) ? tile : -1;
     };
@@ -417,7 +434,7 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
      * them back itself, so no barrier is needed. */
     auto stage_rgba = [&](long long n) {
         if (!want_rbg || n >= count) return;
-        const int code = lst[n];
+        const int code = code_at(n);
         const int tile = code >> 8;
         if (!(code & (1 << 7)) || tile < 0 || tile >= ntiles || !(code & TP_TASK_TEXTURE_BITS)) return;
         int gy0, gx0;
@@ -441,7 +458,7 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     }
 
     for (long long n = blockIdx.x; n < count; n += gridDim.x) {
-        const int code = lst[n];
+        const int code = code_at(n);
         const int tile = tile_of(n);
         const long long n_next = n + gridDim.x;
         cp_async_wait_all();
