@@ -128,7 +128,7 @@ int tp_reset_lpf(void);
  * No counterpart in the reference (its launches are fixed).  The stage kernels
  * walk their work items with grid-stride loops over a grid capped at
  * ctas_per_sm x the SM count; the cap sets how many tiles each CTA takes in
- * turn.  0 restores the built-in value (convert 8, correlate 6, textures 4).
+ * turn.  0 restores the built-in value (convert 8, correlate 8, textures 4).
  * Process-wide, read at every launch (a CUDA graph keeps the shape it was
  * captured with).  tile_processor_gpu_b200.autotune picks the value by timing
  * the caller's workload. */
@@ -293,6 +293,25 @@ int tp_generate_RBGA_noalloc(const tp_geometry *g,
                              int dust_remove, int keep_weights,
                              size_t texture_rbga_stride, float *texture_tiles,
                              tp_stream_t stream);
+
+/* generate_RBGA for one band of tile rows of a frame split across GPUs.  No
+ * counterpart in the reference (one GPU per frame there).  Every task passed
+ * in is marked as a texture tile, so it sets its neighbours' bits and the
+ * window of interest, but only tiles of rows [row_first, row_last) are listed
+ * and accumulated; passing the band's rows plus one tile row above and below
+ * gives the band's tiles the neighbour bits, border classes and alpha fade they
+ * have in the whole frame.  The RGBA image is relative to the band's window of
+ * interest (woi[1] = row_first - 1 unless row_first is the frame's first row);
+ * the 8 pixel rows the band's last tile row adds below row_last * 8 belong to
+ * the next band, which adds them to its own (one strip exchange).  The
+ * parameters the reference passes through unused (is_lwir, diff_threshold,
+ * min_agree, keep_weights) are left out. */
+int tp_generate_RBGA_rows(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                          int *num_texture_tiles, int *woi, int width, int height, float *const *clt,
+                          const float *port_offsets, int colors, float min_shot, float scale_shot,
+                          float diff_sigma, float weight0, float weight1, float weight2, int dust_remove,
+                          size_t texture_rbga_stride, float *texture_tiles, int row_first, int row_last,
+                          tp_stream_t stream);
 
 /* ---- the whole hot path for one frame ------------------------------------------
  * No single counterpart in the reference: it runs convert_correct_tiles,

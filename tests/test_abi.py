@@ -124,11 +124,11 @@ def test_rejects_bad_arguments(native):
 def test_launch_shapes(native):
     """Grid caps of the stage kernels: defaults, set, reset, bounds."""
     from tile_processor_gpu_b200 import _native as N, autotune as A
-    assert [A.get_shape(k) for k in ("convert", "correlate", "textures")] == [8, 6, 4]
+    assert [A.get_shape(k) for k in ("convert", "correlate", "textures")] == [8, 8, 4]
     A.set_shape("correlate", 12)
     assert A.get_shape("correlate") == 12
     A.reset()
-    assert A.get_shape("correlate") == 6
+    assert A.get_shape("correlate") == 8
     for kernel, v in ((3, 4), (-1, 4), (0, 33), (0, -1)):
         assert _code(lambda: N.call("tp_set_launch_shape", kernel, v)) == N.TP_ERR_ARG
     assert _code(lambda: N.call("tp_get_launch_shape", 7)) == N.TP_ERR_ARG

@@ -60,6 +60,8 @@ SIGNATURES = {
                          _I, _S, _P, _P],
     "tp_generate_RBGA_noalloc": [_G, _P, _I, _I, _I, _P, _P, _I, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, _I, _S,
                                  _P, _P],
+    "tp_generate_RBGA_rows": [_G, _P, _I, _P, _P, _P, _I, _I, _P, _P, _I, _F, _F, _F, _F, _F, _F, _I, _S, _P,
+                              _I, _I, _P],
     "tp_process_frame": [_G, _P, _P, _P, _S, _P, _I, _I, _I, _F, _F, _F, _F, _I, _S, _P, _P, _F, _F, _F, _F, _F,
                          _F, _I, _P, _P, _P, _S, _P, _P, _P],
     "tp_disparity_fit": [_G, _P, _S, _I, _S, _P, _P, _I, _I, _P, _P, _P],

@@ -156,13 +156,27 @@ def generate_RBGA(geom, gpu_tasks, num_tiles, gpu_texture_indices, num_texture_t
                   gpu_clt, gpu_port_offsets, colors, is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold,
                   min_agree, weight0, weight1, weight2, dust_remove, keep_weights, texture_rbga_stride,
                   gpu_texture_tiles, stream=None):
-    """List + clear + 8 overlap-add passes into the RGBA image (generate_RBGA)."""
+    """List + clear + one overlap-add pass per tile parity into the RGBA image (generate_RBGA)."""
     _native.call("tp_generate_RBGA", geom.ptr, _dptr(gpu_tasks), int(num_tiles), _dptr(gpu_texture_indices),
                  _dptr(num_texture_tiles), _dptr(woi), int(width), int(height), _parr(gpu_clt),
                  _dptr(gpu_port_offsets), int(colors), int(is_lwir), float(min_shot), float(scale_shot),
                  float(diff_sigma), float(diff_threshold), float(min_agree), float(weight0), float(weight1),
                  float(weight2), int(dust_remove), int(keep_weights), int(texture_rbga_stride),
                  _dptr(gpu_texture_tiles), _stream(stream))
+
+
+def generate_RBGA_rows(geom, gpu_tasks, num_tiles, gpu_texture_indices, num_texture_tiles, woi, width, height,
+                       gpu_clt, gpu_port_offsets, colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2,
+                       dust_remove, texture_rbga_stride, gpu_texture_tiles, row_first, row_last, stream=None):
+    """generate_RBGA for the band of tile rows [row_first, row_last) of a frame
+    split across GPUs: every task marks its tile, only the band's tiles are
+    listed and accumulated (pass the band's tasks plus one tile row above and
+    below; sharding.band_tasks)."""
+    _native.call("tp_generate_RBGA_rows", geom.ptr, _dptr(gpu_tasks), int(num_tiles), _dptr(gpu_texture_indices),
+                 _dptr(num_texture_tiles), _dptr(woi), int(width), int(height), _parr(gpu_clt),
+                 _dptr(gpu_port_offsets), int(colors), float(min_shot), float(scale_shot), float(diff_sigma),
+                 float(weight0), float(weight1), float(weight2), int(dust_remove), int(texture_rbga_stride),
+                 _dptr(gpu_texture_tiles), int(row_first), int(row_last), _stream(stream))
 
 
 def generate_RBGA_noalloc(geom, gpu_tasks, num_tiles, width, height, gpu_clt, gpu_port_offsets, colors, is_lwir,

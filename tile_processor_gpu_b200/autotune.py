@@ -11,7 +11,7 @@ from . import _native
 
 KERNELS = {"convert": 0, "correlate": 1, "textures": 2}
 CANDIDATES = {"convert": (2, 3, 4, 6, 8, 12, 16),
-              "correlate": (3, 4, 6, 9, 12, 16),
+              "correlate": (4, 6, 8, 12, 16),
               "textures": (2, 3, 4, 8, 12)}
 
 

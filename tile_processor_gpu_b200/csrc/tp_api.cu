@@ -9,6 +9,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <math.h>
 #include <atomic>
 #include <mutex>
@@ -100,7 +101,7 @@ unsigned grid_for(long long items, int items_per_block, int sms, int per_sm)
 
 /* grid caps of the stage kernels in CTAs per SM (0 = the built-in value) */
 std::atomic<int> g_shape[TP_SHAPE_COUNT];
-const int g_shape_default[TP_SHAPE_COUNT] = {8, 6, 4};
+const int g_shape_default[TP_SHAPE_COUNT] = {8, 8, 4};
 
 int shape_per_sm(int which)
 {
@@ -363,8 +364,10 @@ int tp_imclt_rbg_all(const tp_geometry *g, const float *clt_one_cam, float *rbg,
     return TP_OK;
 }
 
-int tp_prepare_texture_list(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
-                            int *num_texture_tiles, int *woi, int width, int height, tp_stream_t stream)
+/* prepare_texture_list listing only tiles of rows [row_first, row_last) */
+static int prepare_list(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                        int *num_texture_tiles, int *woi, int width, int height, int row_first, int row_last,
+                        tp_stream_t stream)
 {
     tp::Geom gd;
     int rc = check_geometry(g, &gd);
@@ -386,10 +389,17 @@ int tp_prepare_texture_list(const tp_geometry *g, tp_task *tasks, int num_tiles,
     if (bt) {
         tp::k_mark_neighbor_tiles<<<bt, 256, 0, s>>>(tasks, num_tiles, texture_indices, woi, gd.TX, gd.TY, cap);
         tp::k_gen_texture_list<<<bt, 256, 0, s>>>(tasks, num_tiles, texture_indices, num_texture_tiles, woi,
-                                                  gd.TX, gd.TX * (gd.TYA >> 2), cap);
+                                                  gd.TX, gd.TX * (gd.TYA >> 2), cap, row_first, row_last);
     }
     tp::k_woi_finalize<<<1, 32, 0, s>>>(woi);
     return cuda_status(cudaGetLastError(), "prepare_texture_list launch");
+}
+
+int tp_prepare_texture_list(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                            int *num_texture_tiles, int *woi, int width, int height, tp_stream_t stream)
+{
+    return prepare_list(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height, 0, INT_MAX,
+                        stream);
 }
 
 int tp_clear_texture_rbga(const tp_geometry *g, int texture_width, int texture_slice_height,
@@ -409,14 +419,12 @@ int tp_clear_texture_rbga(const tp_geometry *g, int texture_width, int texture_s
     return cuda_status(cudaGetLastError(), "clear_texture_rbga launch");
 }
 
-int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
-                     int *num_texture_tiles, int *woi, int width, int height, float *const *clt,
-                     const float *port_offsets, int colors, int is_lwir, float min_shot, float scale_shot,
-                     float diff_sigma, float diff_threshold, float min_agree, float weight0, float weight1,
-                     float weight2, int dust_remove, int keep_weights, size_t texture_rbga_stride,
-                     float *texture_tiles, tp_stream_t stream)
+static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                         int *num_texture_tiles, int *woi, int width, int height, float *const *clt,
+                         const float *port_offsets, int colors, float min_shot, float scale_shot, float diff_sigma,
+                         float weight0, float weight1, float weight2, int dust_remove, size_t texture_rbga_stride,
+                         float *texture_tiles, int row_first, int row_last, tp_stream_t stream)
 {
-    (void)is_lwir; (void)diff_threshold; (void)min_agree; (void)keep_weights;
     tp::Geom gd;
     int rc = check_geometry(g, &gd);
     if (rc) return rc;
@@ -427,8 +435,8 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
     if (!clt || !port_offsets || !texture_tiles) return fail(TP_ERR_ARG, "NULL clt / port_offsets / output");
     if (texture_rbga_stride < (size_t)(gd.TX + 1) * 8)
         return fail(TP_ERR_ARG, "texture_rbga_stride %zu < (tilesx + 1) * 8", texture_rbga_stride);
-    if ((rc = tp_prepare_texture_list(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height,
-                                      stream)))
+    if ((rc = prepare_list(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height, row_first,
+                           row_last, stream)))
         return rc;
     cudaStream_t s = (cudaStream_t)stream;
     int sms;
@@ -451,6 +459,33 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
             texture_rbga_stride, texture_tiles, 0, nullptr);
     }
     return cuda_status(cudaGetLastError(), "generate_RBGA launch");
+}
+
+int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                     int *num_texture_tiles, int *woi, int width, int height, float *const *clt,
+                     const float *port_offsets, int colors, int is_lwir, float min_shot, float scale_shot,
+                     float diff_sigma, float diff_threshold, float min_agree, float weight0, float weight1,
+                     float weight2, int dust_remove, int keep_weights, size_t texture_rbga_stride,
+                     float *texture_tiles, tp_stream_t stream)
+{
+    (void)is_lwir; (void)diff_threshold; (void)min_agree; (void)keep_weights;
+    return generate_rbga(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height, clt,
+                         port_offsets, colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2,
+                         dust_remove, texture_rbga_stride, texture_tiles, 0, INT_MAX, stream);
+}
+
+int tp_generate_RBGA_rows(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                          int *num_texture_tiles, int *woi, int width, int height, float *const *clt,
+                          const float *port_offsets, int colors, float min_shot, float scale_shot,
+                          float diff_sigma, float weight0, float weight1, float weight2, int dust_remove,
+                          size_t texture_rbga_stride, float *texture_tiles, int row_first, int row_last,
+                          tp_stream_t stream)
+{
+    if (row_first < 0 || row_last < row_first)
+        return fail(TP_ERR_ARG, "tile rows [%d, %d)", row_first, row_last);
+    return generate_rbga(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height, clt,
+                         port_offsets, colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2,
+                         dust_remove, texture_rbga_stride, texture_tiles, row_first, row_last, stream);
 }
 
 int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *const *kernels, float *const *images,

@@ -133,7 +133,7 @@ __device__ __forceinline__ void corr_job(const float *a, const float *b, int cst
     __syncwarp(gm);
 }
 
-__global__ void __launch_bounds__(128, 3) k_correlate2D(Geom g, float *const *clt, int colors,
+__global__ void __launch_bounds__(128, 4) k_correlate2D(Geom g, float *const *clt, int colors,
                                                         float scale0, float scale1, float scale2,
                                                         float fat_zero, long long num_corr_tiles,
                                                         const int *__restrict__ corr_indices,

@@ -76,16 +76,19 @@ __global__ void k_mark_neighbor_tiles(tp_task *tasks, int num_tiles, const int *
  * the start of their quarter of the buffer, border lists down from its end.
  * Slots are claimed with one atomic per (warp, sub-list). */
 __global__ void k_gen_texture_list(const tp_task *__restrict__ tasks, int num_tiles, int *idx,
-                                   int *counts, const int *woi, int TX, int quarter, long long cap)
+                                   int *counts, const int *woi, int TX, int quarter, long long cap,
+                                   int row_first, int row_last)
 {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int slot = -1, entry = 0, head = 0;
     if (n < num_tiles) {
         const int task = tasks[n].task & TP_TASK_TEXTURE_BITS;
-        if (task) {
-            const int cxy = tasks[n].txy;
-            const int x = cxy & 0xffff, y = cxy >> 16;
+        const int cxy = tasks[n].txy;
+        const int x = cxy & 0xffff, y = cxy >> 16;
+        /* tiles outside [row_first, row_last) stay marked (they set their
+         * neighbours' bits and the window) but are not listed */
+        if (task && y >= row_first && y < row_last) {
             const int border = (x == woi[0]) || (y == woi[1]) || (x == TX - 1) || (y == woi[3]);
             slot = 0;
             if (x & 1) { head += quarter; slot += 2; }
