@@ -718,10 +718,11 @@ def run_b200(args, rank, world, local, pg):
 # --------------------------------------------------------------------------- #
 # CPU implementation (the FP64 port of the reference's tile math)
 # --------------------------------------------------------------------------- #
-def cpu_pipeline(sample_tiles, seed=0):
+def cpu_pipeline(sample_tiles, seed=0, size=None):
     """A bounded sample of the workload for the CPU port: a crop of the same
-    seeded scene, sized to about `sample_tiles` tiles, through all three
-    stages (the per-tile work does not depend on the frame size)."""
+    seeded scene, sized to about `sample_tiles` tiles (or a whole frame of
+    `size` = (w, h)), through all three stages (the per-tile work does not
+    depend on the frame size)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from tile_processor_gpu_b200 import synth
@@ -729,6 +730,8 @@ def cpu_pipeline(sample_tiles, seed=0):
     rng = np.random.default_rng(seed)
     w = WIDTH
     h = max(32, min(HEIGHT, (sample_tiles // (WIDTH // 8)) * 8))
+    if size is not None:
+        w, h = size
     geom = synth.geometry(w, h, image_rows=h + 16)
     imgs, disp = synth.plane_scene(rng, w, h, disparity=(0.0, 64.0), texture="detail")
     dstride = w + 64
@@ -758,9 +761,17 @@ def cpu_baseline(sample_tiles, min_seconds=10.0, max_reps=5):
         reps += 1
     dt = (time.perf_counter() - t) / reps
     frames = ntiles / ((WIDTH // 8) * (HEIGHT // 8))
+    # the small configuration (a whole 256x256 quad frame, 1,024 tiles) as well
+    _, small_step, _, _ = cpu_pipeline(0, size=(256, 256))
+    small_step()
+    t = time.perf_counter()
+    for _ in range(3):
+        small_step()
+    small_ms = (time.perf_counter() - t) / 3 * 1e3
     return {"value": round(frames / dt, 5), "unit": UNIT, "cores": O.get_threads(), "kind": "port",
             "sample": "%s of the scene through all three stages, FP64, %d rep(s); frames = tiles / 78,408" % (
-                what, reps)}
+                what, reps),
+            "full_frame_ms": round(1e3 * dt / frames, 1), "small_256x256_ms": round(small_ms, 2)}
 
 
 def run_reference(args, rank, world, pg):
