@@ -4,13 +4,15 @@ The camera fusion of the texture stage (tile_combine_rgba) takes discrete
 choices -- best and second-best camera, worst camera for dust removal -- from
 weights that can be equal to within float32 rounding.  Near such a tie, any
 two correct implementations that round differently (the reference's
-butterflies with 6-digit constants, this library's matrix transforms, the
-FP64 oracle) may legitimately produce different outputs.
+butterflies with 6-digit constants, this library's butterflies with exact
+constants, the FP64 oracle's matrix products) may legitimately produce
+different outputs.
 
 A texture output is called *stable* when the FP64 oracle reproduces it to
 1e-5 (relative to the slice maximum) both after its input CLT is perturbed by
 random relative noise of 1e-6 -- about the size of the differences between
-float32 evaluations -- and when its window tables are rounded to 6 decimals
+float32 evaluations -- in each of eight trials, and when its window tables
+are rounded to 6 decimals
 as the reference's printed tables are (the 1/sin^4 edge weighting of the
 fusion amplifies that rounding, 3.8e-5 at the first tap).  The oracle keeps
 the camera weights in float32, as the reference does, so exact float ties
@@ -19,6 +21,14 @@ on stable outputs; the fraction of unstable ones is bounded.  On smooth
 scenes the colour and alpha slices are stable almost everywhere; the port
 weights of high-dynamic-range scenes, whose weights sit near the 1e-4 floor,
 are the ill-conditioned ones.
+
+Random trials sample the near-tie pixels rather than enumerate them: on the
+HDR test scene the flagged fraction grows from 0.008% of the colour outputs
+with two trials to 0.015% with eight and 0.018% with sixteen.  The smallest
+relative gap between the weights behind each discrete choice (the oracle's
+`margin`) does not separate them either: exact ties at the 1e-4 floor are
+common and mostly harmless (10% of a smooth scene's pixels have a gap below
+1e-5, of which a few hundredths of a percent move under perturbation).
 """
 import numpy as np
 
@@ -34,7 +44,7 @@ def texture_outputs(oracle, case, clt64, idx, keep_weights=0, colors=3):
     return out.reshape(len(idx), ns, 16, 16)
 
 
-def unstable_mask(oracle, case, clt64, idx, keep_weights=0, colors=3, trials=2, seed=100):
+def unstable_mask(oracle, case, clt64, idx, keep_weights=0, colors=3, trials=8, seed=100):
     """(unstable [n][ns][16][16] bool per slice, oracle outputs [n][ns][16][16])"""
     base = texture_outputs(oracle, case, clt64, idx, keep_weights, colors)
     scale = np.maximum(np.abs(base).max(axis=(0, 2, 3)), 1e-300)[None, :, None, None]

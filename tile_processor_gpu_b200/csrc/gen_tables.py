@@ -9,6 +9,13 @@ closed form, in double precision, and printed as a correctly rounded float:
   dctiv_nodiverg / dstiv_nodiverg (src/dtt8x8.cuh:621-745);
 * ``TP_DCT2 / TP_DST2``   DCT-II / DST-II scaled by 1/2 for every k, the
   reference's dttii_shared_mem_nonortho (src/dtt8x8.cuh:382-463);
+* ``TP_DCT4_PRE / TP_DCT4_POST``  the twiddles of the 8-point DCT-IV through
+  a 4-point complex transform: (cos, sin)(pi m / 8), m = 0..3, and
+  0.5 (cos, sin)(pi (4p+1) / 32), p = 0..3 (tp_common.cuh dct4_fast);
+* ``TP_DCT2_FAST``         the constants of the 8-point DCT-II split into a
+  4-point DCT-II and a 4-point DCT-IV: 0.5 cos(pi/4), 0.5 cos(pi/8),
+  0.5 cos(3 pi/8), cos(pi/4), 0.5 (cos, sin)(pi/16), 0.5 (cos, sin)(5 pi/16)
+  (tp_common.cuh dct2_fast);
 * ``TP_HWIN / TP_HWINC``  sin / cos (pi (2n+1) / 32), n = 0..15: the 16-tap
   lapped window and its quadrature (HWINDOW, src/TileProcessor.cuh:374-383);
 * ``TP_RIND``             window sample -> DTT index of the fold / unfold
@@ -110,6 +117,15 @@ def main():
     names = ["TP_DCT4", "TP_DST4", "TP_DCT2", "TP_DST2"]
     for kind, name in enumerate(names):
         out.append(fmt_matrix(name, dtt(kind)))
+    pre = [[math.cos(math.pi * m / 8.0), math.sin(math.pi * m / 8.0)] for m in range(4)]
+    post = [[0.5 * math.cos(math.pi * (4 * p + 1) / 32.0), 0.5 * math.sin(math.pi * (4 * p + 1) / 32.0)]
+            for p in range(4)]
+    out.append(fmt_matrix("TP_DCT4_PRE", pre))
+    out.append(fmt_matrix("TP_DCT4_POST", post))
+    q = math.pi
+    d2 = [0.5 * math.cos(q / 4), 0.5 * math.cos(q / 8), 0.5 * math.cos(3 * q / 8), math.cos(q / 4),
+          0.5 * math.cos(q / 16), 0.5 * math.sin(q / 16), 0.5 * math.cos(5 * q / 16), 0.5 * math.sin(5 * q / 16)]
+    out.append("#define TP_DCT2_FAST_INIT {" + ", ".join(f32(v) for v in d2) + "}")
     hw = [math.sin(math.pi * (2 * n + 1) / 32.0) for n in range(16)]
     hwc = [math.cos(math.pi * (2 * n + 1) / 32.0) for n in range(16)]
     out.append("#define TP_HWIN_INIT {" + ", ".join(f32(v) for v in hw) + "}")

@@ -4,9 +4,9 @@
  * Work decomposition used by every kernel: one 8x8 transform job (one tile,
  * camera and color) is owned by a group of 8 consecutive lanes of a warp.
  * Lane l of the group holds one row or one column of each 8x8 quadrant in
- * registers, so the 8-point transforms along the held direction are plain
- * register matrix-vector products (the DTT matrices are __constant__ operands
- * of the FMAs); the other direction goes through one 8x9 shared-memory
+ * registers, so the 8-point transforms along the held direction are
+ * butterflies in registers (dct4_fast, dct2_fast); the other direction goes
+ * through one 8x9 shared-memory
  * transpose per quadrant, padded so that both the row writes and the column
  * reads are bank-conflict free.  Groups never wait on each other: the only
  * synchronisation is __syncwarp on the group's 8-lane mask, so a block has no
@@ -21,10 +21,6 @@
 namespace tp {
 
 /* ---- constant tables (generated by gen_tables.py) -------------------------- */
-__device__ __constant__ float c_dct4[8][8] = TP_DCT4_INIT;
-__device__ __constant__ float c_dst4[8][8] = TP_DST4_INIT;
-__device__ __constant__ float c_dct2[8][8] = TP_DCT2_INIT;
-__device__ __constant__ float c_dst2[8][8] = TP_DST2_INIT;
 __device__ __constant__ float c_hwin[16] = TP_HWIN_INIT;
 __device__ __constant__ float c_hwinc[16] = TP_HWINC_INIT;
 __device__ __constant__ int c_rind[16] = TP_RIND_INIT;
@@ -78,23 +74,90 @@ __device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-/* y[k] = sum_n M[k][n] x[n] with M a constant table */
-template <int KIND>
-__device__ __forceinline__ void dtt8(const float x[8], float y[8])
+/* 8-point DCT-IV (SINE false) or DST-IV (SINE true) with the tables' scale,
+ * y[k] = 0.5 sum_n x[n] cos|sin(pi (2k+1)(2n+1) / 32), through a 4-point
+ * complex transform: with a_m = x[2m], b_m = x[7-2m] (swapped for the sine,
+ * as DST-IV x = (-1)^k DCT-IV of x reversed), z_m = (a_m - i b_m)
+ * e^{i pi m / 8}, Z_p = sum_m z_m i^{mp} and Y_p = 0.5 e^{i pi (4p+1) / 32}
+ * Z_p: y[2p] = Re Y_p, y[7-2p] = Im Y_p (negated for the sine).  44
+ * operations against the 64 multiply-adds of the matrix product. */
+template <bool SINE>
+__host__ __device__ __forceinline__ void dct4_fast(const float x[8], float y[8])
 {
+    constexpr float pre[4][2] = TP_DCT4_PRE_INIT;
+    constexpr float post[4][2] = TP_DCT4_POST_INIT;
+    float zr[4], zi[4];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        float a = 0.0f;
-#pragma unroll
-        for (int n = 0; n < 8; n++) {
-            float m = KIND == 0 ? c_dct4[k][n] : KIND == 1 ? c_dst4[k][n] : KIND == 2 ? c_dct2[k][n] : c_dst2[k][n];
-            a = __fmaf_rn(m, x[n], a);
+    for (int m = 0; m < 4; m++) {
+        const float a = SINE ? x[7 - 2 * m] : x[2 * m];
+        const float b = SINE ? x[2 * m] : x[7 - 2 * m];
+        if (m == 0) {
+            zr[0] = a;
+            zi[0] = -b;
+        } else {
+            zr[m] = fmaf(a, pre[m][0], b * pre[m][1]);
+            zi[m] = fmaf(a, pre[m][1], -(b * pre[m][0]));
         }
-        y[k] = a;
+    }
+    const float s02r = zr[0] + zr[2], s02i = zi[0] + zi[2], d02r = zr[0] - zr[2], d02i = zi[0] - zi[2];
+    const float s13r = zr[1] + zr[3], s13i = zi[1] + zi[3], d13r = zr[1] - zr[3], d13i = zi[1] - zi[3];
+    const float Zr[4] = {s02r + s13r, d02r - d13i, s02r - s13r, d02r + d13i};
+    const float Zi[4] = {s02i + s13i, d02i + d13r, s02i - s13i, d02i - d13r};
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+        const float yr = fmaf(Zr[p], post[p][0], -(Zi[p] * post[p][1]));
+        const float yi = fmaf(Zr[p], post[p][1], Zi[p] * post[p][0]);
+        y[2 * p] = yr;
+        y[7 - 2 * p] = SINE ? -yi : yi;
     }
 }
 
-/* Same with the matrix chosen at run time (group-uniform). */
+/* 8-point DCT-II (SINE false) or DST-II (SINE true) with the tables' scale,
+ * y[k] = 0.5 sum_n x[n] cos(pi (2n+1) k / 16) | sin(pi (2n+1) (k+1) / 16):
+ * the even outputs are the 4-point DCT-II of u_n = x_n + x_{7-n}, the odd
+ * ones the 4-point DCT-IV of v_n = x_n - x_{7-n} (through a 2-point complex
+ * transform, as in dct4_fast); the DST-II is the DCT-II of (-1)^n x_n with
+ * the outputs in reverse order.  36 operations against 64. */
+template <bool SINE>
+__host__ __device__ __forceinline__ void dct2_fast(const float xin[8], float y[8])
+{
+    constexpr float K[8] = TP_DCT2_FAST_INIT;
+    float x[8];
+#pragma unroll
+    for (int n = 0; n < 8; n++) x[n] = (SINE && (n & 1)) ? -xin[n] : xin[n];
+    const float u0 = x[0] + x[7], u1 = x[1] + x[6], u2 = x[2] + x[5], u3 = x[3] + x[4];
+    const float v0 = x[0] - x[7], v1 = x[1] - x[6], v2 = x[2] - x[5], v3 = x[3] - x[4];
+    const float w0 = u0 + u3, w1 = u1 + u2, d0 = u0 - u3, d1 = u1 - u2;
+    float r[8];
+    r[0] = 0.5f * (w0 + w1);
+    r[4] = K[0] * (w0 - w1);
+    r[2] = fmaf(d0, K[1], d1 * K[2]);
+    r[6] = fmaf(d0, K[2], -(d1 * K[1]));
+    /* 4-point DCT-IV of v: z0 = v0 - i v3, z1 = (v2 - i v1) e^{i pi / 4} */
+    const float z1r = K[3] * (v2 + v1), z1i = K[3] * (v2 - v1);
+    const float p0r = v0 + z1r, p0i = z1i - v3; /* Z_0 = z0 + z1 */
+    const float p1r = v0 - z1r, p1i = -v3 - z1i; /* Z_1 = z0 - z1 */
+    r[1] = fmaf(p0r, K[4], -(p0i * K[5]));
+    r[7] = fmaf(p0r, K[5], p0i * K[4]);
+    r[5] = fmaf(p1r, K[6], -(p1i * K[7]));
+    r[3] = fmaf(p1r, K[7], p1i * K[6]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) y[k] = SINE ? r[7 - k] : r[k];
+}
+
+/* y[k] = sum_n M[k][n] x[n] for the four 8-point transforms of the tables:
+ * DCT-IV / DST-IV (KIND 0 / 1) through dct4_fast, DCT-II / DST-II (KIND 2 /
+ * 3) through dct2_fast */
+template <int KIND>
+__device__ __forceinline__ void dtt8(const float x[8], float y[8])
+{
+    if constexpr (KIND == 0 || KIND == 1)
+        dct4_fast<KIND == 1>(x, y);
+    else
+        dct2_fast<KIND == 3>(x, y);
+}
+
+/* Same with the transform chosen at run time (group-uniform). */
 __device__ __forceinline__ void dtt8_sel(int sine, int dtt2, const float x[8], float y[8])
 {
     if (dtt2) {
