@@ -23,7 +23,6 @@ namespace tp {
 /* ---- constant tables (generated by gen_tables.py) -------------------------- */
 __device__ __constant__ float c_hwin[16] = TP_HWIN_INIT;
 __device__ __constant__ float c_hwinc[16] = TP_HWINC_INIT;
-__device__ __constant__ int c_rind[16] = TP_RIND_INIT;
 /* Tables that lanes index by their own row / column live in global memory
  * and are read through the read-only data cache: the lanes of a warp then
  * fetch distinct words in one pass, where the constant cache would serialise
@@ -155,16 +154,6 @@ __device__ __forceinline__ void dtt8(const float x[8], float y[8])
         dct4_fast<KIND == 1>(x, y);
     else
         dct2_fast<KIND == 3>(x, y);
-}
-
-/* Same with the transform chosen at run time (group-uniform). */
-__device__ __forceinline__ void dtt8_sel(int sine, int dtt2, const float x[8], float y[8])
-{
-    if (dtt2) {
-        if (sine) dtt8<3>(x, y); else dtt8<2>(x, y);
-    } else {
-        if (sine) dtt8<1>(x, y); else dtt8<0>(x, y);
-    }
 }
 
 /* 8x8 transpose inside an 8-lane group through an 8x9 buffer: lane l
