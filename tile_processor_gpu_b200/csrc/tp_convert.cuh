@@ -214,7 +214,7 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
 
 /* Warp w of the grid-stride loop handles tasks 4*(w/12) .. +3 for camera
  * (w%12)%4 and color (w%12)/4. */
-__global__ void __launch_bounds__(256, 2) k_convert_correct_tiles(
+__global__ void __launch_bounds__(256, 3) k_convert_correct_tiles(
     Geom g, size_t dstride, float *const *kernel_offsets, float *const *kernels,
     float *const *images, const tp_task *__restrict__ tasks, float *const *clt, int num_tiles,
     int lpf_mask)
