@@ -16,6 +16,12 @@ closed form, in double precision, and printed as a correctly rounded float:
   4-point DCT-II and a 4-point DCT-IV: 0.5 cos(pi/4), 0.5 cos(pi/8),
   0.5 cos(3 pi/8), cos(pi/4), 0.5 (cos, sin)(pi/16), 0.5 (cos, sin)(5 pi/16)
   (tp_common.cuh dct2_fast);
+* ``TP_TEX_TFAC / TP_TEX_MFAC / TP_TEX_WND2 / TP_TEX_WI``  per-pixel factors
+  of the texture kernel, computed from the float TP_HWIN values in float32
+  arithmetic in the device's operation order (so they equal what the kernel
+  would compute): tfac[r][c] = (0.25 / w[c]) / w[r], mfac[r][c] = (0.5 w[r])
+  (0.5 w[c]) ([16][17], column 16 zero), wnd2 = w[r]^2 w[c]^2 and
+  wi = 1 / wnd2 ([256]);
 * ``TP_HWIN / TP_HWINC``  sin / cos (pi (2n+1) / 32), n = 0..15: the 16-tap
   lapped window and its quadrature (HWINDOW, src/TileProcessor.cuh:374-383);
 * ``TP_RIND``             window sample -> DTT index of the fold / unfold
@@ -100,6 +106,28 @@ def alpha_fade():
     return out
 
 
+def texture_factors(hw):
+    """The texture kernel's per-pixel tables in float32, operation by operation."""
+    import numpy as np
+    f = np.float32
+    w = [f(float(f32(v)[:-1])) for v in hw]  # the float the compiler makes of each printed literal
+    tfac = [[f(0.0)] * 17 for _ in range(16)]
+    mfac = [[f(0.0)] * 17 for _ in range(16)]
+    for r in range(16):
+        for c in range(16):
+            tfac[r][c] = (f(0.25) / w[c]) / w[r]
+            mfac[r][c] = (f(0.5) * w[r]) * (f(0.5) * w[c])
+    hsq = [w[i] * w[i] for i in range(16)]
+    sym8 = lambda i: (i ^ 15) if (i & 8) else i
+    wnd2 = [hsq[sym8(px >> 4)] * hsq[sym8(px & 15)] for px in range(256)]
+    wi = [f(1.0) / v for v in wnd2]
+    lines = []
+    for name, vals in (("TP_TEX_TFAC", [v for row in tfac for v in row]), ("TP_TEX_MFAC", [v for row in mfac for v in row]),
+                       ("TP_TEX_WND2", wnd2), ("TP_TEX_WI", wi)):
+        lines.append("#define %s_INIT {" % name + ", ".join("%.9ef" % float(v) for v in vals) + "}")
+    return lines
+
+
 def rind(n):
     return n + 4 if n < 4 else (11 - n if n < 12 else n - 12)
 
@@ -127,6 +155,7 @@ def main():
           0.5 * math.cos(q / 16), 0.5 * math.sin(q / 16), 0.5 * math.cos(5 * q / 16), 0.5 * math.sin(5 * q / 16)]
     out.append("#define TP_DCT2_FAST_INIT {" + ", ".join(f32(v) for v in d2) + "}")
     hw = [math.sin(math.pi * (2 * n + 1) / 32.0) for n in range(16)]
+    out.extend(texture_factors(hw))
     hwc = [math.cos(math.pi * (2 * n + 1) / 32.0) for n in range(16)]
     out.append("#define TP_HWIN_INIT {" + ", ".join(f32(v) for v in hw) + "}")
     out.append("#define TP_HWINC_INIT {" + ", ".join(f32(v) for v in hwc) + "}")

@@ -101,7 +101,7 @@ unsigned grid_for(long long items, int items_per_block, int sms, int per_sm)
 
 /* grid caps of the stage kernels in CTAs per SM (0 = the built-in value) */
 std::atomic<int> g_shape[TP_SHAPE_COUNT];
-const int g_shape_default[TP_SHAPE_COUNT] = {8, 8, 4};
+const int g_shape_default[TP_SHAPE_COUNT] = {8, 8, 5};
 
 int shape_per_sm(int which)
 {
@@ -621,7 +621,8 @@ int tp_mlp_colsum(int rows, int cols, int ld, const float *x, float scale, float
     if (rows < 0 || cols < 0 || ld < cols) return fail(TP_ERR_ARG, "colsum %d x %d ld %d", rows, cols, ld);
     if (!cols) return TP_OK;
     if ((rows && !x) || !out) return fail(TP_ERR_ARG, "NULL colsum operand");
-    tp::k_colsum<<<(cols + 127) / 128, 128, 0, (cudaStream_t)stream>>>(rows, cols, ld, x, scale, out);
+    tp::k_colsum<<<(cols + 31) / 32, dim3(32, tp::kColLanes), 0, (cudaStream_t)stream>>>(rows, cols, ld, x, scale,
+                                                                                        out);
     return cuda_status(cudaGetLastError(), "mlp_colsum launch");
 }
 

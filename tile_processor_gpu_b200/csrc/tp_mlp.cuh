@@ -222,15 +222,26 @@ __global__ void k_gelu_backward(long long n, int cols, int ld, const float *__re
     }
 }
 
-/* out[c] = scale * sum over rows of x[r][c] (one thread per column, fixed order) */
-__global__ void k_colsum(int rows, int cols, int ld, const float *__restrict__ x, float scale,
-                         float *__restrict__ out)
+/* out[c] = scale * sum over rows of x[r][c].  Block (32, kColLanes): 32
+ * columns, each summed by kColLanes threads over rows lane, lane + kColLanes,
+ * ... and the lanes' partial sums added in a fixed tree order, so the
+ * result does not depend on scheduling. */
+constexpr int kColLanes = 16;
+__global__ void __launch_bounds__(32 * kColLanes) k_colsum(int rows, int cols, int ld, const float *__restrict__ x,
+                                                           float scale, float *__restrict__ out)
 {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
+    __shared__ float part[kColLanes][33];
+    const int c = blockIdx.x * 32 + threadIdx.x, lane = threadIdx.y;
     float s = 0.0f;
-    for (int r = 0; r < rows; r++) s += x[(size_t)r * ld + c];
-    out[c] = s * scale;
+    if (c < cols)
+        for (int r = lane; r < rows; r += kColLanes) s += x[(size_t)r * ld + c];
+    part[lane][threadIdx.x] = s;
+    __syncthreads();
+    for (int h = kColLanes / 2; h > 0; h >>= 1) {
+        if (lane < h) part[lane][threadIdx.x] += part[lane + h][threadIdx.x];
+        __syncthreads();
+    }
+    if (lane == 0 && c < cols) out[c] = part[0][threadIdx.x] * scale;
 }
 
 /* Gaussian NLL of out[r] = [d, s] against target[r] = truth - plain, with the

@@ -4,8 +4,8 @@
  * :3847-4017, debayer_shot / debayer :4019-4199 and tile_combine_rgba
  * :4202-4665).
  *
- * One 96-thread block (three warps) per listed tile (grid-stride), four
- * blocks per SM.  The block's next tile is staged one tile ahead with
+ * One 96-thread block (three warps) per listed tile (grid-stride), five
+ * blocks per SM (128 registers, 45 KB of shared memory each).  The block's next tile is staged one tile ahead with
  * asynchronous copies: its CLT (into a bank-padded buffer, issued once the
  * current CLT has been read) and, per thread, the RGBA pixels that thread
  * will update.  Per (camera, color) job one 8-lane group, working only with
@@ -46,6 +46,15 @@ __device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
  *   mfac[r][c] = (0.5 w[r]) (0.5 w[c])    windowed tile M = mfac * d
  * with w the half-sine window, in the rounding order of the per-pixel form. */
 constexpr int kFac = 16 * 17;
+/* The same factors, and the squared window at each of the 256 pixels with its
+ * reciprocal, as read-only tables in global memory for k_textures (values
+ * bit-identical to the float expressions above and in the kernel's fusion,
+ * generated by gen_tables.py); the lanes read them through the read-only
+ * cache, which leaves the kernel's shared memory to its tiles. */
+__device__ float d_tex_tfac[kFac] = TP_TEX_TFAC_INIT;
+__device__ float d_tex_mfac[kFac] = TP_TEX_MFAC_INIT;
+__device__ float d_tex_wnd2[256] = TP_TEX_WND2_INIT;
+__device__ float d_tex_wi[256] = TP_TEX_WI_INIT;
 __device__ __forceinline__ void fill_unfold_factors(float *tfac, float *mfac, int tid, int nthreads)
 {
     for (int i = tid; i < 256; i += nthreads) {
@@ -327,7 +336,7 @@ __device__ __forceinline__ void stage_clt(float *const *cp, bool al16, int tile,
     }
 }
 
-__global__ void __launch_bounds__(kTexThreads, 4) k_textures(
+__global__ void __launch_bounds__(kTexThreads, 5) k_textures(
     Geom g, const int *__restrict__ woi, float *const *clt, long long num_texture_tiles,
     const int *__restrict__ list, const int *__restrict__ dev_counts, int count_slot, int list_cap,
     int border_quarter, const float *__restrict__ port_offsets, TextureParams p,
@@ -339,11 +348,8 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     float *s_x = s_t + 12 * kJob;      /* transposes, then the debayered tiles D            */
     float *s_c = s_x + 12 * kTB4;      /* the tile's CLT, staged one tile ahead             */
     float *s_r = s_c + 12 * kCltJob;   /* RGBA pixels under the tile, [slice][256]          */
-    __shared__ float s_hsq[16];
     __shared__ float *s_cp[4];
     __shared__ float s_pd2r[6], s_chw[3];
-    __shared__ float s_tfac[kFac], s_mfac[kFac];
-    __shared__ float s_wnd2[256], s_wi[256]; /* squared window at each pixel, and its reciprocal */
 
     const int tid = threadIdx.x;
     const int l = tid & 7, grp = tid >> 3;
@@ -351,17 +357,6 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
     const int colors = p.colors;
     const int njobs = 4 * colors;
     const float ksigma = (float)(1.0 / (2.0 * (double)p.diff_sigma * (double)p.diff_sigma));
-    fill_unfold_factors(s_tfac, s_mfac, tid, kTexThreads);
-    if (tid < 16) {
-        const float s = c_hwin[tid];
-        s_hsq[tid] = s * s;
-    }
-    __syncthreads();
-    for (int px = tid; px < 256; px += kTexThreads) {
-        const float w2 = s_hsq[sym8(px >> 4)] * s_hsq[sym8(px & 15)];
-        s_wnd2[px] = w2;
-        s_wi[px] = __frcp_rn(w2);
-    }
     if (tid < 4) s_cp[tid] = clt[tid];
     if (tid == 0) {
         int k = 0;
@@ -480,10 +475,10 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
             if (colors > 1) {
                 /* T -> s_t, then the debayered D -> s_x (the transpose
                  * buffer, free once the unfold has read it) */
-                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[color], xj, nullptr, tj, s_tfac, nullptr, l, gm);
+                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[color], xj, nullptr, tj, d_tex_tfac, nullptr, l, gm);
                 debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
             } else {
-                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[3], xj, tj, nullptr, nullptr, s_mfac, l, gm);
+                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[3], xj, tj, nullptr, nullptr, d_tex_mfac, l, gm);
             }
         }
         __syncthreads();
@@ -503,7 +498,7 @@ __global__ void __launch_bounds__(kTexThreads, 4) k_textures(
         for (int px = tid; px < 256; px += kTexThreads) {
             const int r = px >> 4, c = px & 15;
             const int e = JT(r, c);
-            const float wnd2 = s_wnd2[px], wi = s_wi[px];
+            const float wnd2 = __ldg(&d_tex_wnd2[px]), wi = __ldg(&d_tex_wi[px]);
             float o[12];
             if (colors == 3)
                 combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, wnd2, wi, p.dust_remove,
