@@ -78,7 +78,7 @@ __device__ __forceinline__ void fill_unfold_factors(float *tfac, float *mfac, in
  * tout may be NULL (with its factor table). */
 __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *mout,
                                                  float *tout, const float *tfac, const float *mfac, int l,
-                                                 unsigned gm)
+                                                 unsigned gm, int hswap = 0)
 {
     float a[4][8]; /* pixel-domain row l of each quadrant */
 #pragma unroll
@@ -99,8 +99,12 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
     }
     /* the two output rows folding onto row l, and their vertical signs
      * (rows 0-3: +,+; 4-7: -,+; 8-11: -,+; 12-15: -,-) */
+    /* hswap (odd groups of a warp in k_textures) writes the two rows in the
+     * other order: with job buffers 280 floats apart, the four groups' rows
+     * of one store then fall in disjoint banks */
 #pragma unroll 1
-    for (int h = 0; h < 2; h++) {
+    for (int hh = 0; hh < 2; hh++) {
+        const int h = hh ^ hswap;
         const int r = (l >= 4) ? (h ? 11 - l : l - 4) : (h ? l + 12 : 11 - l);
         const int rq = r >> 2;
         const bool n01 = rq != 0, n23 = rq == 3;
@@ -475,10 +479,10 @@ __global__ void __launch_bounds__(kTexThreads, 5) k_textures(
             if (colors > 1) {
                 /* T -> s_t, then the debayered D -> s_x (the transpose
                  * buffer, free once the unfold has read it) */
-                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[color], xj, nullptr, tj, d_tex_tfac, nullptr, l, gm);
+                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[color], xj, nullptr, tj, d_tex_tfac, nullptr, l, gm, grp & 1);
                 debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
             } else {
-                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[3], xj, tj, nullptr, nullptr, d_tex_mfac, l, gm);
+                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[3], xj, tj, nullptr, nullptr, d_tex_mfac, l, gm, grp & 1);
             }
         }
         __syncthreads();
