@@ -81,13 +81,16 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
                                                  unsigned gm, int hswap = 0)
 {
     float a[4][8]; /* pixel-domain row l of each quadrant */
+    float f[8];    /* column l of the low-pass filter, shared by the quadrants */
+#pragma unroll
+    for (int m = 0; m < 8; m++) f[m] = lpf ? __ldg(&lpf[m * 8 + l]) : 1.0f;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         float col[8], v[8], row[8];
 #pragma unroll
         for (int m = 0; m < 8; m++) {
             const float x = src[q * 64 + m * 8 + l];
-            col[m] = lpf ? x * __ldg(&lpf[m * 8 + l]) : x;
+            col[m] = lpf ? x * f[m] : x;
         }
         if (q >> 1) dtt8<1>(col, v); else dtt8<0>(col, v);
 #pragma unroll
