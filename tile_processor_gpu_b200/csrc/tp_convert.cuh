@@ -225,8 +225,8 @@ __global__ void __launch_bounds__(256, 3) k_convert_correct_tiles(
     const unsigned gm = group_mask();
     const int warps_total = gridDim.x * (blockDim.x >> 5);
     const int chunks = (num_tiles + 3) >> 2;
-    /* the task fields of this group's job, read one job ahead so that the
-     * load overlaps the previous job */
+    /* the task fields of this group's job, read two jobs ahead so that the
+     * loads overlap the jobs before it */
     auto fetch = [&](int w, int *task, int *txy, float *cx, float *cy) {
         *task = 0;
         if (w >= chunks * 12) return;
@@ -239,13 +239,17 @@ __global__ void __launch_bounds__(256, 3) k_convert_correct_tiles(
         *cx = __ldg(&t->xy[cam][0]);
         *cy = __ldg(&t->xy[cam][1]);
     };
-    /* its kernel tile's offsets (the kernel-tile choice of convert_job) */
+    /* its kernel tile's offsets (the kernel-tile choice of convert_job),
+     * read one job ahead, and the kernel tile itself prefetched into L2
+     * (lane l: bytes 128 l .. 128 l + 127 of the 1 KB tile) */
     auto fetch_extra = [&](int w, float cx, float cy, float ex[6]) {
         const int r = w % 12, color = r >> 2, cam = r & 3;
         const float step_inv = __int_as_float((127 - g.ls) << 23);
         const int ktx = min(g.KH - 1, max(0, __float2int_rn(__fmaf_rn(cx, step_inv, 1.0f))));
         const int kty = min(g.KV - 1, max(0, __float2int_rn(__fmaf_rn(cy, step_inv, 1.0f))));
-        const float *e = kernel_offsets[cam] + (((size_t)ktx + (size_t)kty * g.KH) * 3 + color) * 8;
+        const size_t kidx = ((size_t)ktx + (size_t)kty * g.KH) * 3 + color;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(kernels[cam] + kidx * 256 + l * 32));
+        const float *e = kernel_offsets[cam] + kidx * 8;
         ex[0] = __ldg(e + 0); ex[1] = __ldg(e + 1);
         ex[2] = __ldg(e + 4); ex[3] = __ldg(e + 5);
         ex[4] = __ldg(e + 6); ex[5] = __ldg(e + 7);
@@ -255,6 +259,9 @@ __global__ void __launch_bounds__(256, 3) k_convert_correct_tiles(
     float ncx = 0.0f, ncy = 0.0f, nex[6];
     fetch(w, &ntask, &ntxy, &ncx, &ncy);
     if (ntask) fetch_extra(w, ncx, ncy, nex);
+    int n2task = 0, n2txy = 0;
+    float n2cx = 0.0f, n2cy = 0.0f;
+    fetch(w + warps_total, &n2task, &n2txy, &n2cx, &n2cy);
     for (; w < chunks * 12; w += warps_total) {
         const int chunk = w / 12, r = w - chunk * 12;
         const int color = r >> 2, cam = r & 3;
@@ -263,8 +270,9 @@ __global__ void __launch_bounds__(256, 3) k_convert_correct_tiles(
         float ex[6];
 #pragma unroll
         for (int i = 0; i < 6; i++) ex[i] = nex[i];
-        fetch(w + warps_total, &ntask, &ntxy, &ncx, &ncy);
+        ntask = n2task; ntxy = n2txy; ncx = n2cx; ncy = n2cy;
         if (ntask) fetch_extra(w + warps_total, ncx, ncy, nex);
+        fetch(w + 2 * warps_total, &n2task, &n2txy, &n2cx, &n2cy);
         if (!task) continue;
         const int tx = txy & 0xfff, ty = txy >> 16;
         if (tx >= g.TX || ty < 0 || ty >= g.TY) continue;
