@@ -46,6 +46,12 @@ struct ConvertJob {
     int cam, color;
 };
 
+/* STREAM: out is global memory and takes evict-first stores.  The kernel
+ * writes 963 MB of CLT for a full quad frame, far more than L2 holds, and
+ * later kernels read it back; retaining the stores in L2 would only evict the
+ * kernel tiles and Bayer rows that neighbouring jobs of this kernel still
+ * read. */
+template <bool STREAM = false>
 __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
                                             const float *__restrict__ extra_tab,
                                             const float *__restrict__ kern_tab,
@@ -205,10 +211,17 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
     }
 #pragma unroll
     for (int m = 0; m < 8; m++) {
-        out[m * 8 + l] = cc[m];
-        out[64 + m * 8 + l] = sc[m];
-        out[128 + m * 8 + l] = cs[m];
-        out[192 + m * 8 + l] = ss[m];
+        if constexpr (STREAM) {
+            __stcs(out + m * 8 + l, cc[m]);
+            __stcs(out + 64 + m * 8 + l, sc[m]);
+            __stcs(out + 128 + m * 8 + l, cs[m]);
+            __stcs(out + 192 + m * 8 + l, ss[m]);
+        } else {
+            out[m * 8 + l] = cc[m];
+            out[64 + m * 8 + l] = sc[m];
+            out[128 + m * 8 + l] = cs[m];
+            out[192 + m * 8 + l] = ss[m];
+        }
     }
 }
 
@@ -277,7 +290,7 @@ __global__ void __launch_bounds__(256, 3) k_convert_correct_tiles(
         const int tx = txy & 0xfff, ty = txy >> 16;
         if (tx >= g.TX || ty < 0 || ty >= g.TY) continue;
         float *out = clt[cam] + (((size_t)ty * g.TX + tx) * 3 + color) * 256;
-        convert_job(g, dstride, kernel_offsets[cam], kernels[cam], images[cam], cx, cy, color,
+        convert_job<true>(g, dstride, kernel_offsets[cam], kernels[cam], images[cam], cx, cy, color,
                     lpf_mask, out, tbuf[grp], l, gm, ex);
     }
 }
