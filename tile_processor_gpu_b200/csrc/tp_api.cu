@@ -451,12 +451,28 @@ static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, in
     if ((rc = texture_smem_setup())) return rc;
     /* one pass per tile parity: its inner sub-list, then its border one (the
      * reference runs the four inner passes, then the four border passes;
-     * tiles of one parity never overlap, so a pass needs no ordering) */
+     * tiles of one parity never overlap, so a pass needs no ordering).
+     * Passes after the first are programmatic dependents of the pass before:
+     * their blocks stage their first tile's CLT while that pass drains and
+     * wait for it before touching the RGBA image.  The first pass is an
+     * ordinary launch, as it reads the list the kernels above build. */
+    cudaLaunchAttribute pdl[1];
+    pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    pdl[0].val.programmaticStreamSerializationAllowed = 1;
     for (int parity = 0; parity < 4; parity++) {
         const int *base = texture_indices + parity * quarter;
-        tp::k_textures<<<grid, tp::kTexThreads, tp::kTexSmemBytes, s>>>(
-            gd, woi, clt, 0, base, num_texture_tiles, parity << 1, quarter, -quarter, port_offsets, p,
-            texture_rbga_stride, texture_tiles, 0, nullptr);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(tp::kTexThreads);
+        cfg.dynamicSmemBytes = tp::kTexSmemBytes;
+        cfg.stream = s;
+        cfg.attrs = pdl;
+        cfg.numAttrs = parity > 0 ? 1 : 0;
+        const cudaError_t err = cudaLaunchKernelEx(
+            &cfg, tp::k_textures, gd, (const int *)woi, clt, 0LL, (const int *)base,
+            (const int *)num_texture_tiles, parity << 1, quarter, -quarter, port_offsets, p, texture_rbga_stride,
+            texture_tiles, (size_t)0, (float *)nullptr);
+        if (err != cudaSuccess) return cuda_status(err, "generate_RBGA texture pass launch");
     }
     return cuda_status(cudaGetLastError(), "generate_RBGA launch");
 }

@@ -73,6 +73,15 @@ __device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+/* Programmatic dependent launch.  A kernel launched with programmatic stream
+ * serialisation may start while the launch before it on the stream is still
+ * running: grid_dependency_wait() blocks the calling thread until that grid
+ * has completed and its memory operations are visible (a no-op for an
+ * ordinary launch), and grid_dependents_launch() lets such a dependent grid
+ * be scheduled once every block of this grid has issued it. */
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 /* 8-point DCT-IV (SINE false) or DST-IV (SINE true) with the tables' scale,
  * y[k] = 0.5 sum_n x[n] cos|sin(pi (2k+1)(2n+1) / 32), through a 4-point
  * complex transform: with a_m = x[2m], b_m = x[7-2m] (swapped for the sine,

@@ -449,13 +449,20 @@ __global__ void __launch_bounds__(kTexThreads, 5) k_textures(
         }
     };
 
+    /* the next tile-parity pass may be scheduled on the SM slots this grid
+     * frees as its blocks finish */
+    grid_dependents_launch();
     {
         const long long n0 = blockIdx.x;
         const int t0 = tile_of(n0);
-        if (t0 >= 0) {
-            stage_clt(s_cp, al16, t0, colors, s_c, tid);
-            stage_rgba(n0);
-        }
+        if (t0 >= 0) stage_clt(s_cp, al16, t0, colors, s_c, tid);
+        /* A pass launched as a programmatic dependent of the previous pass
+         * waits here for it: that pass read-modify-writes the RGBA image.
+         * Everything read above (the list and its counts, the window, the
+         * CLT, the port offsets) was complete before the previous pass
+         * started. */
+        grid_dependency_wait();
+        if (t0 >= 0) stage_rgba(n0);
         cp_async_commit();
     }
 
