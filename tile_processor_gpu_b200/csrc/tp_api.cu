@@ -6,6 +6,7 @@
  * stream.  Nothing here allocates, synchronises or copies device data to the
  * host.
  */
+#include <utility>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -364,6 +365,29 @@ int tp_imclt_rbg_all(const tp_geometry *g, const float *clt_one_cam, float *rbg,
     return TP_OK;
 }
 
+/* Launch kern on stream s; with `dependent` as a programmatic dependent of
+ * the launch before it on s (programmatic stream serialisation): the kernel
+ * may be scheduled before that launch has finished and must wait for it
+ * (grid_dependency_wait) before reading anything it writes. */
+extern "C++" {
+template <typename... Params, typename... Args>
+static cudaError_t launch_chained(bool dependent, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                  void (*kern)(Params...), Args &&...args)
+{
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = dependent ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+} /* extern "C++" */
+
 /* prepare_texture_list listing only tiles of rows [row_first, row_last) */
 static int prepare_list(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
                         int *num_texture_tiles, int *woi, int width, int height, int row_first, int row_last,
@@ -379,19 +403,34 @@ static int prepare_list(const tp_geometry *g, tp_task *tasks, int num_tiles, int
         return fail(TP_ERR_ARG, "list extent %dx%d outside %dx%d tiles", width, height, gd.TX, gd.TY);
     cudaStream_t s = (cudaStream_t)stream;
     const long long cap = (long long)gd.TX * gd.TYA;
+    /* the first kernel is an ordinary launch (it follows the caller's work);
+     * each later one is a programmatic dependent of the one before, which it
+     * waits for on entry (chain_entry) */
+    bool dep = false;
+    cudaError_t err = cudaSuccess;
     if (height > 0) {
         dim3 b0((width + 1 + 255) / 256, height, 1);
-        tp::k_clear_texture_list<<<b0, 256, 0, s>>>(texture_indices, width, height, gd.TX, cap);
+        err = launch_chained(dep, b0, 256, 0, s, tp::k_clear_texture_list, texture_indices, width, height, gd.TX,
+                             cap);
+        dep = true;
     }
     const unsigned bt = (unsigned)((num_tiles + 255) / 256);
-    if (bt) tp::k_mark_texture_tiles<<<bt, 256, 0, s>>>(tasks, num_tiles, texture_indices, gd.TX, cap);
-    tp::k_woi_init<<<1, 32, 0, s>>>(woi, num_texture_tiles, gd.TX, gd.TY);
-    if (bt) {
-        tp::k_mark_neighbor_tiles<<<bt, 256, 0, s>>>(tasks, num_tiles, texture_indices, woi, gd.TX, gd.TY, cap);
-        tp::k_gen_texture_list<<<bt, 256, 0, s>>>(tasks, num_tiles, texture_indices, num_texture_tiles, woi,
-                                                  gd.TX, gd.TX * (gd.TYA >> 2), cap, row_first, row_last);
+    if (bt && err == cudaSuccess) {
+        err = launch_chained(dep, bt, 256, 0, s, tp::k_mark_texture_tiles, (const tp_task *)tasks, num_tiles,
+                             texture_indices, gd.TX, cap);
+        dep = true;
     }
-    tp::k_woi_finalize<<<1, 32, 0, s>>>(woi);
+    if (err == cudaSuccess)
+        err = launch_chained(dep, 1, 32, 0, s, tp::k_woi_init, woi, num_texture_tiles, gd.TX, gd.TY);
+    if (bt && err == cudaSuccess)
+        err = launch_chained(true, bt, 256, 0, s, tp::k_mark_neighbor_tiles, tasks, num_tiles,
+                             (const int *)texture_indices, woi, gd.TX, gd.TY, cap);
+    if (bt && err == cudaSuccess)
+        err = launch_chained(true, bt, 256, 0, s, tp::k_gen_texture_list, (const tp_task *)tasks, num_tiles,
+                             texture_indices, num_texture_tiles, (const int *)woi, gd.TX, gd.TX * (gd.TYA >> 2),
+                             cap, row_first, row_last);
+    if (err == cudaSuccess) err = launch_chained(true, 1, 32, 0, s, tp::k_woi_finalize, woi);
+    if (err != cudaSuccess) return cuda_status(err, "prepare_texture_list launch");
     return cuda_status(cudaGetLastError(), "prepare_texture_list launch");
 }
 
@@ -441,37 +480,30 @@ static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, in
     cudaStream_t s = (cudaStream_t)stream;
     int sms;
     if ((rc = sm_count(&sms))) return rc;
+    if ((rc = texture_smem_setup())) return rc;
+    /* The RGBA clear and the four passes continue prepare_list's chain of
+     * programmatic dependents.  The clear waits on entry for the list's last
+     * kernel.  A pass stages its first tile's CLT and reads the list before it
+     * waits for the launch before it (the clear, or the previous pass, which
+     * read-modify-writes the RGBA image): that launch released it only after
+     * its own wait, so the list was complete by then. */
     {
         const int max_rows = (gd.TY + 1) * 8 * (colors + 1);
-        tp::k_clear_rbga<<<grid_for(max_rows, 1, sms, 16), 256, 0, s>>>(woi, colors, 0, 0, texture_rbga_stride,
-                                                                         texture_tiles);
+        const cudaError_t err = launch_chained(true, grid_for(max_rows, 1, sms, 16), 256, 0, s, tp::k_clear_rbga,
+                                               (const int *)woi, colors, 0, 0, texture_rbga_stride, texture_tiles);
+        if (err != cudaSuccess) return cuda_status(err, "generate_RBGA clear launch");
     }
     const int quarter = gd.TX * (gd.TYA >> 2);
     const unsigned grid = grid_for(quarter, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
-    if ((rc = texture_smem_setup())) return rc;
     /* one pass per tile parity: its inner sub-list, then its border one (the
      * reference runs the four inner passes, then the four border passes;
-     * tiles of one parity never overlap, so a pass needs no ordering).
-     * Passes after the first are programmatic dependents of the pass before:
-     * their blocks stage their first tile's CLT while that pass drains and
-     * wait for it before touching the RGBA image.  The first pass is an
-     * ordinary launch, as it reads the list the kernels above build. */
-    cudaLaunchAttribute pdl[1];
-    pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    pdl[0].val.programmaticStreamSerializationAllowed = 1;
+     * tiles of one parity never overlap, so a pass needs no ordering) */
     for (int parity = 0; parity < 4; parity++) {
         const int *base = texture_indices + parity * quarter;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(grid);
-        cfg.blockDim = dim3(tp::kTexThreads);
-        cfg.dynamicSmemBytes = tp::kTexSmemBytes;
-        cfg.stream = s;
-        cfg.attrs = pdl;
-        cfg.numAttrs = parity > 0 ? 1 : 0;
-        const cudaError_t err = cudaLaunchKernelEx(
-            &cfg, tp::k_textures, gd, (const int *)woi, clt, 0LL, (const int *)base,
-            (const int *)num_texture_tiles, parity << 1, quarter, -quarter, port_offsets, p, texture_rbga_stride,
-            texture_tiles, (size_t)0, (float *)nullptr);
+        const cudaError_t err = launch_chained(
+            true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures, gd, (const int *)woi, clt, 0LL,
+            (const int *)base, (const int *)num_texture_tiles, parity << 1, quarter, -quarter, port_offsets, p,
+            texture_rbga_stride, texture_tiles, (size_t)0, (float *)nullptr);
         if (err != cudaSuccess) return cuda_status(err, "generate_RBGA texture pass launch");
     }
     return cuda_status(cudaGetLastError(), "generate_RBGA launch");

@@ -17,9 +17,21 @@
 
 namespace tp {
 
+/* First statements of every kernel of the list / RGBA-clear sequence, which
+ * the host launches as a chain of programmatic dependents: wait for the
+ * launch before (everything it wrote is then visible), and only then let the
+ * next one be scheduled.  A kernel that starts early therefore only ever runs
+ * ahead of its own predecessor, never of the kernels before that. */
+__device__ __forceinline__ void chain_entry()
+{
+    grid_dependency_wait();
+    grid_dependents_launch();
+}
+
 /* marker grid: cols 0..width (inclusive, as the reference), rows 0..height-1 */
 __global__ void k_clear_texture_list(int *idx, int width, int height, int TX, long long cap)
 {
+    chain_entry();
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     const int row = blockIdx.y;
     if (col > width || row >= height) return;
@@ -30,6 +42,7 @@ __global__ void k_clear_texture_list(int *idx, int width, int height, int TX, lo
 __global__ void k_mark_texture_tiles(const tp_task *__restrict__ tasks, int num_tiles, int *idx, int TX,
                                      long long cap)
 {
+    chain_entry();
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= num_tiles) return;
     if (!(tasks[n].task & TP_TASK_TEXTURE_BITS)) return;
@@ -40,6 +53,7 @@ __global__ void k_mark_texture_tiles(const tp_task *__restrict__ tasks, int num_
 
 __global__ void k_woi_init(int *woi, int *counts, int TX, int TY)
 {
+    chain_entry();
     if (threadIdx.x == 0) {
         woi[0] = TX; woi[1] = TY; woi[2] = 0; woi[3] = 0;
     }
@@ -54,6 +68,7 @@ __device__ __forceinline__ int marker_at(const int *idx, long long i, long long 
 __global__ void k_mark_neighbor_tiles(tp_task *tasks, int num_tiles, const int *idx, int *woi, int TX,
                                       int TY, long long cap)
 {
+    chain_entry();
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= num_tiles) return;
     const int task = tasks[n].task;
@@ -79,6 +94,7 @@ __global__ void k_gen_texture_list(const tp_task *__restrict__ tasks, int num_ti
                                    int *counts, const int *woi, int TX, int quarter, long long cap,
                                    int row_first, int row_last)
 {
+    chain_entry();
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int slot = -1, entry = 0, head = 0;
@@ -110,6 +126,7 @@ __global__ void k_gen_texture_list(const tp_task *__restrict__ tasks, int num_ti
 
 __global__ void k_woi_finalize(int *woi)
 {
+    chain_entry();
     if (threadIdx.x == 0) {
         woi[2] += 1 - woi[0];
         woi[3] += 1 - woi[1];
@@ -122,6 +139,7 @@ __global__ void k_woi_finalize(int *woi)
 __global__ void k_clear_rbga(const int *woi, int colors, int texture_width, int slice_height,
                              size_t stride, float *buf)
 {
+    chain_entry();
     int tw = texture_width, rows = slice_height;
     if (woi) {
         tw = (woi[2] + 1) * 8;
