@@ -128,7 +128,7 @@ int tp_reset_lpf(void);
  * No counterpart in the reference (its launches are fixed).  The stage kernels
  * walk their work items with grid-stride loops over a grid capped at
  * ctas_per_sm x the SM count; the cap sets how many tiles each CTA takes in
- * turn.  0 restores the built-in value (convert 8, correlate 8, textures 5).
+ * turn.  0 restores the built-in value (convert 8, correlate 8, textures 7).
  * Process-wide, read at every launch (a CUDA graph keeps the shape it was
  * captured with).  tile_processor_gpu_b200.autotune picks the value by timing
  * the caller's workload. */

@@ -124,7 +124,7 @@ def test_rejects_bad_arguments(native):
 def test_launch_shapes(native):
     """Grid caps of the stage kernels: defaults, set, reset, bounds."""
     from tile_processor_gpu_b200 import _native as N, autotune as A
-    assert [A.get_shape(k) for k in ("convert", "correlate", "textures")] == [8, 8, 5]
+    assert [A.get_shape(k) for k in ("convert", "correlate", "textures")] == [8, 8, 7]
     A.set_shape("correlate", 12)
     assert A.get_shape("correlate") == 12
     A.reset()

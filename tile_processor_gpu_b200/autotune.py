@@ -12,7 +12,7 @@ from . import _native
 KERNELS = {"convert": 0, "correlate": 1, "textures": 2}
 CANDIDATES = {"convert": (2, 3, 4, 6, 8, 12, 16),
               "correlate": (4, 6, 8, 12, 16),
-              "textures": (3, 4, 5, 10, 15)}
+              "textures": (5, 6, 7, 14, 21)}
 
 
 def set_shape(kernel, ctas_per_sm):

@@ -102,7 +102,7 @@ unsigned grid_for(long long items, int items_per_block, int sms, int per_sm)
 
 /* grid caps of the stage kernels in CTAs per SM (0 = the built-in value) */
 std::atomic<int> g_shape[TP_SHAPE_COUNT];
-const int g_shape_default[TP_SHAPE_COUNT] = {8, 8, 5};
+const int g_shape_default[TP_SHAPE_COUNT] = {8, 8, 7};
 
 int shape_per_sm(int which)
 {
@@ -483,7 +483,7 @@ static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, in
     if ((rc = texture_smem_setup())) return rc;
     /* The RGBA clear and the four passes continue prepare_list's chain of
      * programmatic dependents.  The clear waits on entry for the list's last
-     * kernel.  A pass stages its first tile's CLT and reads the list before it
+     * kernel.  A pass prefetches its first tile's CLT and reads the list before it
      * waits for the launch before it (the clear, or the previous pass, which
      * read-modify-writes the RGBA image): that launch released it only after
      * its own wait, so the list was complete by then. */

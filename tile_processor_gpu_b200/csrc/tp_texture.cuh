@@ -4,12 +4,13 @@
  * :3847-4017, debayer_shot / debayer :4019-4199 and tile_combine_rgba
  * :4202-4665).
  *
- * One 96-thread block (three warps) per listed tile (grid-stride), five
- * blocks per SM (128 registers, 45 KB of shared memory each).  The block's next tile is staged one tile ahead with
- * asynchronous copies: its CLT (into a bank-padded buffer, issued once the
- * current CLT has been read) and, per thread, the RGBA pixels that thread
- * will update.  Per (camera, color) job one 8-lane group, working only with
- * __syncwarp on its own buffers:
+ * One 96-thread block (three warps) per listed tile (grid-stride), seven
+ * blocks per SM (80 registers, 27 KB of shared memory each: the tiles T and
+ * D only).  The CLT is read straight from global memory by the inverse
+ * transform; the next tile's CLT and the RGBA rows it will update are
+ * prefetched into L2 while the block works on the current tile.  Per
+ * (camera, color) job one 8-lane group, working only with __syncwarp on its
+ * own buffers:
  *   1. low-pass filter and invert the CLT tile (vertical DCT-IV/DST-IV on the
  *      held column, transpose, horizontal pass on the held row) and unfold it
  *      into the un-windowed tile T (colour) or the windowed tile M (mono);
@@ -316,34 +317,11 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
 /* k_textures block: three warps, one 8-lane group per (camera, colour) job */
 constexpr int kTexThreads = 96;
 /* dynamic shared memory of k_textures, in floats: T (un-windowed tiles),
- * transposes then D (debayered tiles), the staged CLT, the prefetched RGBA */
-constexpr int kTexSmemFloats = 12 * kJob + 12 * kTB4 + 12 * kCltJob + 4 * 256;
+ * transposes then D (debayered tiles) */
+constexpr int kTexSmemFloats = 12 * kJob + 12 * kTB4;
 constexpr size_t kTexSmemBytes = sizeof(float) * kTexSmemFloats;
 
-/* Stage the CLT of one tile (jobs cam * colors + color) into s_c with
- * asynchronous copies: 16-byte chunks when every camera plane is 16-byte
- * aligned, else 4-byte ones.  A camera plane holds the tile's three colours
- * contiguously (768 floats). */
-__device__ __forceinline__ void stage_clt(float *const *cp, bool al16, int tile, int colors, float *s_c, int tid)
-{
-    if (al16 && colors == 3) {
-#pragma unroll
-        for (int i = 0; i < 768 / kTexThreads; i++) {
-            const int k = tid + kTexThreads * i; /* 16-byte chunk of the tile, 0..767 */
-            const int cam = k / 192, w = k - cam * 192;
-            cp_async16(s_c + (cam * 3 + (w >> 6)) * kCltJob + (w & 63) * 4, cp[cam] + (size_t)tile * 768 + w * 4);
-        }
-    } else {
-        const int njobs = 4 * colors;
-        for (int k = tid; k < njobs * 256; k += kTexThreads) {
-            const int job = k >> 8, e = k & 255;
-            const int cam = job / colors, color = job - cam * colors;
-            cp_async4(s_c + job * kCltJob + e, cp[cam] + ((size_t)tile * 3 + color) * 256 + e);
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kTexThreads, 5) k_textures(
+__global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     Geom g, const int *__restrict__ woi, float *const *clt, long long num_texture_tiles,
     const int *__restrict__ list, const int *__restrict__ dev_counts, int count_slot, int list_cap,
     int border_quarter, const float *__restrict__ port_offsets, TextureParams p,
@@ -353,8 +331,6 @@ __global__ void __launch_bounds__(kTexThreads, 5) k_textures(
     extern __shared__ __align__(16) float smem[];
     float *s_t = smem;                 /* un-windowed tiles T (colour) or windowed M (mono) */
     float *s_x = s_t + 12 * kJob;      /* transposes, then the debayered tiles D            */
-    float *s_c = s_x + 12 * kTB4;      /* the tile's CLT, staged one tile ahead             */
-    float *s_r = s_c + 12 * kCltJob;   /* RGBA pixels under the tile, [slice][256]          */
     __shared__ float *s_cp[4];
     __shared__ float s_pd2r[6], s_chw[3];
 
@@ -408,8 +384,6 @@ __global__ void __launch_bounds__(kTexThreads, 5) k_textures(
     if (want_rbg) { wx0 = woi[0]; wy0 = woi[1]; wh = woi[3]; }
     const size_t slice_stride = texture_rbg_stride * (size_t)(wh + 1) * 8;
     __syncthreads();
-    const bool al16 = !((reinterpret_cast<uintptr_t>(s_cp[0]) | reinterpret_cast<uintptr_t>(s_cp[1]) |
-                         reinterpret_cast<uintptr_t>(s_cp[2]) | reinterpret_cast<uintptr_t>(s_cp[3])) & 15);
     const int ntiles = g.TX * g.TY;
     /* list entry -> tile index, or -1 when the entry is not a texture tile */
     auto tile_of = [&](long long n) -> int {
@@ -431,21 +405,30 @@ __global__ void __launch_bounds__(kTexThreads, 5) k_textures(
         if (gy < 0 || gx < 0) return nullptr;
         return texture_rbg + (size_t)gy * texture_rbg_stride + (size_t)gx;
     };
-    /* Thread tid combines pixels tid, tid + 96, tid + 192 (< 256) and owns
-     * them in the RGBA image: it prefetches them for list entry n and reads
-     * them back itself, so no barrier is needed. */
-    auto stage_rgba = [&](long long n) {
+    /* The next tile's inputs are prefetched into L2 while the block works on
+     * the current one: its CLT (one 128-byte line per thread: 24 lines of 768
+     * floats per camera) and the RGBA rows its pixels update (both ends of
+     * each 16-pixel row of each slice).  The RGBA prefetch comes after the
+     * wait for the previous pass, which writes those rows. */
+    auto prefetch_clt = [&](int tile) {
+        const int cam = tid / 24, line = tid - cam * 24;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(s_cp[cam] + (size_t)tile * 768 + line * 32));
+    };
+    auto prefetch_rgba = [&](long long n) {
         if (!want_rbg || n >= count) return;
         const int code = code_at(n);
         const int tile = code >> 8;
         if (!(code & (1 << 7)) || tile < 0 || tile >= ntiles || !(code & TP_TASK_TEXTURE_BITS)) return;
         int gy0, gx0;
         rgba_origin(tile, &gy0, &gx0);
-#pragma unroll
-        for (int px = tid; px < 256; px += kTexThreads) {
-            const float *b = rgba_at(gy0, gx0, px);
-            if (!b) continue;
-            for (int sl = 0; sl <= colors; sl++) cp_async4(s_r + sl * 256 + px, b + (size_t)sl * slice_stride);
+        const int r = tid & 15, sl = tid >> 4; /* row r of slice sl */
+        if (sl <= colors) {
+            const float *b = rgba_at(gy0, gx0, r * 16);
+            if (b) {
+                b += (size_t)sl * slice_stride;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(b));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(b + 15));
+            }
         }
     };
 
@@ -455,30 +438,27 @@ __global__ void __launch_bounds__(kTexThreads, 5) k_textures(
     {
         const long long n0 = blockIdx.x;
         const int t0 = tile_of(n0);
-        if (t0 >= 0) stage_clt(s_cp, al16, t0, colors, s_c, tid);
+        if (t0 >= 0) prefetch_clt(t0);
         /* A pass launched as a programmatic dependent of the previous pass
          * waits here for it: that pass read-modify-writes the RGBA image.
          * Everything read above (the list and its counts, the window, the
          * CLT, the port offsets) was complete before the previous pass
          * started. */
         grid_dependency_wait();
-        if (t0 >= 0) stage_rgba(n0);
-        cp_async_commit();
+        if (t0 >= 0) prefetch_rgba(n0);
     }
 
     for (long long n = blockIdx.x; n < count; n += gridDim.x) {
         const int code = code_at(n);
         const int tile = tile_of(n);
         const long long n_next = n + gridDim.x;
-        cp_async_wait_all();
-        __syncthreads(); /* staged CLT visible; the previous tile's buffers free */
+        __syncthreads(); /* the previous tile's buffers free */
         if (tile < 0) {
             const int tn = tile_of(n_next);
             if (tn >= 0) {
-                stage_clt(s_cp, al16, tn, colors, s_c, tid);
-                stage_rgba(n_next);
+                prefetch_clt(tn);
+                prefetch_rgba(n_next);
             }
-            cp_async_commit();
             continue;
         }
 
@@ -489,18 +469,18 @@ __global__ void __launch_bounds__(kTexThreads, 5) k_textures(
             if (colors > 1) {
                 /* T -> s_t, then the debayered D -> s_x (the transpose
                  * buffer, free once the unfold has read it) */
-                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[color], xj, nullptr, tj, d_tex_tfac, nullptr, l, gm, grp & 1);
+                imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[color], xj, nullptr, tj,
+                                 d_tex_tfac, nullptr, l, gm, grp & 1);
                 debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
             } else {
-                imclt_unfold_job(s_c + grp * kCltJob, d_lpf[3], xj, tj, nullptr, nullptr, d_tex_mfac, l, gm, grp & 1);
+                imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[3], xj, tj, nullptr,
+                                 nullptr, d_tex_mfac, l, gm, grp & 1);
             }
         }
         __syncthreads();
         {
-            /* the CLT of this block's next tile lands while this one finishes */
             const int tn = tile_of(n_next);
-            if (tn >= 0) stage_clt(s_cp, al16, tn, colors, s_c, tid);
-            cp_async_commit();
+            if (tn >= 0) prefetch_clt(tn);
         }
 
         /* ---- stages 3-4: fuse the four cameras at the thread's pixels and
@@ -534,13 +514,13 @@ __global__ void __launch_bounds__(kTexThreads, 5) k_textures(
                     for (int sl = 0; sl < 4; sl++) {
                         if (sl > colors) break;
                         const float v = (nbr != TP_TASK_TEXTURE_BITS) ? o[sl] * f : o[sl];
-                        b[(size_t)sl * slice_stride] = s_r[sl * 256 + px] + v;
+                        float *q = b + (size_t)sl * slice_stride;
+                        *q = *q + v;
                     }
                 }
             }
         }
-        stage_rgba(n_next);
-        cp_async_commit();
+        prefetch_rgba(n_next);
     }
 }
 
