@@ -133,6 +133,9 @@ def test_launch_shapes(native):
         assert _code(lambda: N.call("tp_set_launch_shape", kernel, v)) == N.TP_ERR_ARG
     assert _code(lambda: N.call("tp_get_launch_shape", 7)) == N.TP_ERR_ARG
     assert A.get_shape("convert") == 8
+    # the tuner never steps off the built-in shape: each default is a candidate
+    for k in A.KERNELS:
+        assert A.get_shape(k) in A.CANDIDATES[k]
 
 
 def test_zero_work_is_ok_without_gpu(native):
