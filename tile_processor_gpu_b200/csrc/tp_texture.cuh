@@ -439,11 +439,11 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
         const long long n0 = blockIdx.x;
         const int t0 = tile_of(n0);
         if (t0 >= 0) prefetch_clt(t0);
-        /* A pass launched as a programmatic dependent of the previous pass
-         * waits here for it: that pass read-modify-writes the RGBA image.
-         * Everything read above (the list and its counts, the window, the
-         * CLT, the port offsets) was complete before the previous pass
-         * started. */
+        /* A pass launched as a programmatic dependent of the launch before it
+         * (the RGBA clear, or the previous tile-parity pass) waits here for
+         * it: that launch writes the RGBA image.  Everything read above (the
+         * list and its counts, the window, the CLT, the port offsets) was
+         * complete before that launch let this one start. */
         grid_dependency_wait();
         if (t0 >= 0) prefetch_rgba(n0);
     }
