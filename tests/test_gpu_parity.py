@@ -531,3 +531,59 @@ def test_clear_texture_rbga_extent(native, width, height, stride):
     assert np.all(b[:height, :cols] == 0.0)
     assert np.all(b[:height, cols:] == 3.0)
     assert np.all(b[height:] == 3.0)
+
+
+def test_generate_rbga_back_to_back(frames, clts):
+    """Two generate_RBGA calls queued on one stream with no synchronisation
+    between them and one set of texture-list buffers, the second with a
+    sparser task set and another window of interest: each RGBA image and
+    window equals the same call run alone, bit for bit.  Inside a call the
+    list kernels, the RGBA clear and the four passes are programmatic
+    dependent launches; the first kernel of a call is an ordinary launch, so
+    a call never starts before the previous one has finished."""
+    import torch
+    R = _R()
+    from tile_processor_gpu_b200 import api
+    fr, _ = _corr_case(frames, clts, "B512plane")
+    c = fr.case
+    p = R.TEX
+    sparse = c.tasks.copy()
+    tx, ty = sparse["txy"] & 0xffff, sparse["txy"] >> 16
+    drop = (ty < 3) | (tx < 5) | ((tx + ty) % 7 == 0)
+    sparse["task"][drop] &= ~0xf  # no texture for these tiles
+    stride = (c.TX + 1) * 8 + 40
+    rows = (c.TY + 1) * 8 * (p["colors"] + 1)
+    args = (p["colors"], p["is_lwir"], p["min_shot"], p["scale_shot"], p["diff_sigma"], p["diff_threshold"],
+            p["min_agree"], p["weight0"], p["weight1"], p["weight2"], p["dust_remove"], 0)
+
+    def lists():
+        return (torch.zeros(c.TX * c.TYA + 256, dtype=torch.int32, device="cuda"),
+                torch.zeros(8, dtype=torch.int32, device="cuda"), torch.zeros(4, dtype=torch.int32, device="cuda"))
+
+    def image():
+        return torch.full((rows + 8, stride), 3.0, dtype=torch.float32, device="cuda")
+
+    def call(tasks, lst, out):
+        t = api.tasks_to_device(tasks, "cuda")
+        idx, cnt, woi = lst
+        api.generate_RBGA(fr.g, t, c.num_tiles, idx, cnt, woi, c.TX, c.TY, fr.p_clt, fr.port_offsets, *args,
+                          stride, out)
+        return t
+
+    alone = []
+    for tasks in (c.tasks, sparse):
+        lst, out = lists(), image()
+        call(tasks, lst, out)
+        torch.cuda.synchronize()
+        alone.append((out.cpu().numpy(), lst[2].cpu().numpy()))
+    assert not np.array_equal(alone[0][1], alone[1][1])  # the windows differ
+
+    lst, o1, o2 = lists(), image(), image()
+    keep = [call(c.tasks, lst, o1)]
+    woi1 = lst[2].clone()
+    keep.append(call(sparse, lst, o2))
+    torch.cuda.synchronize()
+    assert np.array_equal(woi1.cpu().numpy(), alone[0][1])
+    assert np.array_equal(lst[2].cpu().numpy(), alone[1][1])
+    assert np.array_equal(o1.cpu().numpy(), alone[0][0])
+    assert np.array_equal(o2.cpu().numpy(), alone[1][0])
