@@ -15,9 +15,14 @@ through the public API with host buffers: each step copies the frame's four
 images from pinned host memory and reads the correlation tiles and the RGBA
 texture back.
 
+One step is `--frames-per-step` passes of that frame (48 by default), so the
+timed region of a default run lasts a few seconds and the clock samples taken
+during it mean something.
+
 `--impl reference` times the CPU implementation (the FP64 port of the
-reference's tile math, all host threads) on a bounded sample of the same
-workload.
+reference's tile math, all host threads), one whole 2592x1936 frame per step,
+and beside it the reference's own CUDA kernels rebuilt for sm_100a on the same
+frame (`reference_kernels`, when that build is present).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 """
@@ -48,14 +53,33 @@ WORKLOAD = ("full-frame quad 2592x1936 Bayer (78,408 tiles): forward CLT + aberr
             "6-pair correlation (15x15), texture list + overlapped RGBA texture")
 
 
+TILES = (WIDTH // 8) * (HEIGHT // 8)
+CORR_TILES = 6 * TILES
+FRAMES_PER_STEP = 48
+L2_NOTE = ("per-frame working set 3.7 GB (images, touched kernel tables, CLT, correlations, RGBA) > 126 MB L2: "
+           "no flush")
 # dense 8x8 mat-vec flops per tile of each stage (2 flop per MAC)
 FLOPS_PER_TILE = {"convert": 75776, "correlate": 92016, "texture": 149304}
 # FP32 SIMT: 148 SMs x 128 lanes x 2 flop x 1.965 GHz
 FP32_NOMINAL_TFLOPS = 74.4
-# DRAM bytes of each stage of one frame of this workload from an ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum summed over the stage's
-# launches; profiles/launch_list_2592x1936_quad.md)
-TRAFFIC = {"convert": 1380.4e6, "correlate": 1356.6e6, "texture": 1570.1e6}
+
+
+def bench_config(world):
+    """the workload both arms report (identical in both)"""
+    return {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "tiles": TILES, "corr_tiles": CORR_TILES,
+            "parallelism": "frame replicas x%d" % world, "l2": L2_NOTE}
+
+
+def dram_traffic():
+    """DRAM bytes per frame of each stage from the ncu capture recorded with
+    the package (a capture, not a measurement of this run)"""
+    path = os.path.join(ROOT, "tile_processor_gpu_b200", "data", "dram_traffic.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return d["bytes_per_frame"], "ncu capture: " + d["command"]
+    except (OSError, ValueError, KeyError):
+        return {}, None
 
 
 def peaks():
@@ -212,7 +236,8 @@ class BatchedFrames:
                 ef[..., 3] -= oy
                 extras.append(ef.contiguous().view(-1))
             self.frames.append(dict(
-                g=api.Geometry.from_dict(geom), TX=TX, TY=TY, dstride=dstride, size=(w, h),
+                g=api.Geometry.from_dict(geom), geom=geom, tasks_np=tasks_np, activity=float(mask.mean()),
+                TX=TX, TY=TY, dstride=dstride, size=(w, h),
                 num_tiles=int(tasks_np.size), num_corr=int(idx.size), tasks=api.tasks_to_device(tasks_np, dev),
                 corr_idx=torch.from_numpy(idx).to(dev), images=images, kernels=kernels, extras=extras,
                 p_images=api.PointerArray(images), p_kernels=api.PointerArray(kernels),
@@ -511,32 +536,35 @@ def run_b200(args, rank, world, local, pg):
         shapes = autotune.tune_stages({"convert": pipe.convert, "correlate": pipe.correlate,
                                        "textures": pipe.texture})
     frame_shapes = {k: autotune.get_shape(k) for k in autotune.KERNELS}
-    for _ in range(args.warmup):
+    for _ in range(args.warmup * args.frames_per_step):
         pipe.step()
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
     ev = {s: [] for s in pipe.STAGES}
+    F = args.frames_per_step
     barrier(pg)
     torch.cuda.synchronize()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record(stream)
     for _ in range(args.steps):
-        for s in pipe.STAGES:
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            getattr(pipe, s)()
-            b.record(stream)
-            ev[s].append((a, b))
+        for _ in range(F):
+            for s in pipe.STAGES:
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                getattr(pipe, s)()
+                b.record(stream)
+                ev[s].append((a, b))
     t_end.record(stream)
     torch.cuda.synchronize()
     barrier(pg)
     clocks = sampler.stop()
     ms = t_start.elapsed_time(t_end)
     ms_max = max_over_ranks(pg, ms)
-    stage_ms = {s: sum(a.elapsed_time(b) for a, b in ev[s]) / args.steps for s in pipe.STAGES}
+    frames_timed = args.steps * F
+    stage_ms = {s: sum(a.elapsed_time(b) for a, b in ev[s]) / frames_timed for s in pipe.STAGES}
 
     # the same frame through tp_process_frame (fused per tile), reported beside
     fused_steps = max(3, min(args.steps, 10))
@@ -683,16 +711,16 @@ def run_b200(args, rank, world, local, pg):
     algo = pipe.algorithmic_bytes()
     dom = max(stage_ms, key=stage_ms.get)
     achieved = algo[dom] / (stage_ms[dom] * 1e-3) / 1e9
-    fps = world * args.steps / (ms_max * 1e-3)
+    fps = world * frames_timed / (ms_max * 1e-3)
     flops = FLOPS_PER_TILE[dom] * pipe.num_tiles
+    traffic, traffic_source = dram_traffic()
     out = {
         "metric": METRIC, "value": round(fps, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plane scene, centred PSF kernels)",
-        "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "tiles": pipe.num_tiles,
-                   "corr_tiles": pipe.num_corr, "parallelism": "frame replicas x%d" % world,
-                   "path": "tp_convert_correct_tiles + tp_correlate2D + tp_generate_RBGA",
-                   "l2": "per-step working set %.2f GB > 126 MB L2 (no flush)" % (sum(algo.values()) / 1e9)},
+        "config": bench_config(world),
+        "frames_per_step": F, "ms_per_frame": round(ms_max / frames_timed, 4),
+        "path": "tp_convert_correct_tiles + tp_correlate2D + tp_generate_RBGA",
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "fused_frame_ms": round(fused_ms, 4),
         "graph_frame_ms": graph_ms,
@@ -701,28 +729,30 @@ def run_b200(args, rank, world, local, pg):
         "launch_shapes": shapes or frame_shapes,
         "roofline": {"bound": "hbm", "kernel": "k_textures (%s stage)" % dom, "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
-                     "algorithmic_bytes": int(algo[dom]), "traffic": int(TRAFFIC[dom]) if dom in TRAFFIC else None,
+                     "algorithmic_bytes": int(algo[dom]), "traffic": int(traffic[dom]) if dom in traffic else None,
+                     "traffic_source": traffic_source,
                      "fp32_simt": {"flops": int(flops), "achieved_tflops": round(flops / (stage_ms[dom] * 1e-3) / 1e12, 2),
                                    "nominal_peak_tflops": FP32_NOMINAL_TFLOPS}},
         "e2e": {"value": round(world / (e2e_ms * 1e-3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "frames": e2e_steps,
                 "overlap": "two frames in flight: copy-in, compute, copy-out streams"},
-        "gpu_launches": int(args.steps * sum(pipe.LAUNCHES.values())),
+        "gpu_launches": int(frames_timed * sum(pipe.LAUNCHES.values())),
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args.cpu_sample_tiles)
+        out["cpu_baseline"], out["parity"] = cpu_baseline(args.cpu_sample_tiles)
     return out
 
 
 # --------------------------------------------------------------------------- #
 # CPU implementation (the FP64 port of the reference's tile math)
 # --------------------------------------------------------------------------- #
-def cpu_pipeline(sample_tiles, seed=0, size=None):
+def cpu_pipeline(sample_tiles, seed=100, size=None):
     """A bounded sample of the workload for the CPU port: a crop of the same
     seeded scene, sized to about `sample_tiles` tiles (or a whole frame of
     `size` = (w, h)), through all three stages (the per-tile work does not
-    depend on the frame size)."""
+    depend on the frame size).  With seed 100 and the full size this is the
+    frame the B200 arm's rank 0 runs.  Returns the inputs and a step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from tile_processor_gpu_b200 import synth
@@ -740,73 +770,232 @@ def cpu_pipeline(sample_tiles, seed=0, size=None):
     kern, extra = synth.kernel_tables(rng, geom, pool=256, zero_extra=True, psf_offset=0.0)
     tasks = synth.tasks_grid(geom, rng, jitter=0.0, disparity=disp, disparity_error=DISPARITY_ERROR)
     corr_idx = synth.corr_indices_fast(tasks, geom)
-    TX, TY, _ = synth.tiles(geom)
+    TX, TY, TYA = synth.tiles(geom)
 
     def step():
         clt = O.convert_correct_tiles(geom, extra, kern, pitched, dstride, tasks)
         O.correlate2D(geom, clt, 3, .25, .25, .5, FAT_ZERO, corr_idx, (2 * CORR_RADIUS + 1) ** 2, CORR_RADIUS)
         O.generate_RBGA(geom, tasks, TX, TY, clt, synth.PORT_OFFSETS, (TX + 1) * 8, (TY + 1) * 8 * 4 + 8)
 
-    return O, step, int(tasks.size), "%dx%d crop (%d tiles)" % (w, h, tasks.size)
+    full = (w, h) == (WIDTH, HEIGHT)
+    return dict(O=O, step=step, ntiles=int(tasks.size), geom=geom, pitched=pitched, kern=kern, extra=extra,
+                tasks=tasks, corr_idx=corr_idx, TX=TX, TY=TY, TYA=TYA, dstride=dstride,
+                port_offsets=synth.PORT_OFFSETS,
+                what=("the whole %dx%d frame (%d tiles)" if full else "%dx%d crop (%d tiles)") % (w, h, tasks.size))
+
+
+def sample_parity(S):
+    """This library's three calls on the CPU sample's inputs, checked against
+    the FP64 oracle: the CLT from the same inputs, the correlations and the
+    overlapped RGBA image from this library's CLT (the tests' rule: texture
+    pixels on stable outputs only, oracle/conditioning.py).  Relative to the
+    oracle's largest magnitude per array / per RGBA slice."""
+    import torch
+    import conditioning
+    from tile_processor_gpu_b200 import api
+    O, geom, TX, TY = S["O"], S["geom"], S["TX"], S["TY"]
+    dev = "cuda"
+    pa = api.PointerArray
+    g = api.Geometry.from_dict(geom)
+    images = [torch.from_numpy(S["pitched"][c]).to(dev) for c in range(4)]
+    kernels = [torch.from_numpy(np.ascontiguousarray(S["kern"][c])).to(dev) for c in range(4)]
+    extras = [torch.from_numpy(np.ascontiguousarray(S["extra"][c])).to(dev) for c in range(4)]
+    tasks = api.tasks_to_device(S["tasks"], dev)
+    n, idx = S["ntiles"], S["corr_idx"]
+    clt = [torch.zeros(TX * TY * 768, dtype=torch.float32, device=dev) for _ in range(4)]
+    api.convert_correct_tiles(g, pa(extras), pa(kernels), pa(images), tasks, pa(clt), S["dstride"], n, 0)
+    corrs = torch.zeros((len(idx), 225), dtype=torch.float32, device=dev)
+    api.correlate2D(g, pa(clt), 3, .25, .25, .5, FAT_ZERO, len(idx), torch.from_numpy(idx).to(dev), 225,
+                    CORR_RADIUS, corrs)
+    stride, rows = (TX + 1) * 8, (TY + 1) * 8 * 4
+    rgba = torch.zeros((rows, stride), dtype=torch.float32, device=dev)
+    lst = torch.zeros(TX * S["TYA"], dtype=torch.int32, device=dev)
+    cnt = torch.zeros(8, dtype=torch.int32, device=dev)
+    woi_d = torch.zeros(4, dtype=torch.int32, device=dev)
+    t = TEXTURE
+    po = np.ascontiguousarray(S["port_offsets"], np.float32).reshape(-1)
+    api.generate_RBGA(g, tasks, n, lst, cnt, woi_d, TX, TY, pa(clt), torch.from_numpy(po).to(dev), t["colors"],
+                      t["is_lwir"], t["min_shot"], t["scale_shot"], t["diff_sigma"], t["diff_threshold"],
+                      t["min_agree"], t["weight0"], t["weight1"], t["weight2"], t["dust_remove"], 0, stride, rgba)
+    torch.cuda.synchronize()
+    clt_h = [c.cpu().numpy() for c in clt]
+    rel = lambda a, b: float(np.abs(np.asarray(a, np.float64) - b).max() / max(np.abs(b).max(), 1e-300))
+    want = O.convert_correct_tiles(geom, S["extra"], S["kern"], S["pitched"], S["dstride"], S["tasks"])
+    e_clt = max(rel(clt_h[c], want[c]) for c in range(4))
+    c64 = [x.astype(np.float64) for x in clt_h]
+    co = O.correlate2D(geom, c64, 3, .25, .25, .5, FAT_ZERO, idx, 225, CORR_RADIUS)
+    e_corr = rel(corrs.cpu().numpy(), co)
+    o, _, _, _, _ = O.generate_RBGA(geom, S["tasks"], TX, TY, clt_h, po, stride, rows + 8)
+    woi = woi_d.cpu().numpy()
+    h, w = (woi[3] + 1) * 8, (woi[2] + 1) * 8
+    txy = S["tasks"]["txy"].astype(np.int64)
+    tiles = (txy & 0xFFFF) + (txy >> 16) * TX
+    bad, _ = conditioning.unstable_tiles(O, geom, po, clt_h, tiles)
+    m = conditioning.unstable_image_mask(bad.any(axis=1), tiles << 8, woi, TX, (h, w), 4)
+    sl = lambda a: a[:4 * h, :w].reshape(4, h, w)[None]
+    per = conditioning.stable_errors(sl(rgba.cpu().numpy()), sl(o), sl(~m))
+    names = ("r", "b", "g", "alpha")
+    return {"against": "FP64 oracle (CPU restatement of the reference's tile math)", "sample": S["what"],
+            "clt_max_rel": float("%.3g" % e_clt), "corr_max_rel": float("%.3g" % e_corr),
+            "texture": {"rule": "overlapped RGBA on pixels whose tiles the oracle's conditioning probe finds stable "
+                                "(1e-6 input perturbations, 6-digit window tables); error relative to the slice "
+                                "maximum",
+                        "slices": {nm: {k: float("%.3g" % v) for k, v in r.items()} for nm, r in zip(names, per)}}}
 
 
 def cpu_baseline(sample_tiles, min_seconds=10.0, max_reps=5):
     """The port on all host threads: repeat the sample until about
-    `min_seconds` of CPU work (at most `max_reps` repetitions)."""
-    O, step, ntiles, what = cpu_pipeline(sample_tiles)
+    `min_seconds` of CPU work (at most `max_reps` repetitions).  Also returns
+    the parity of this library against the oracle on the same sample."""
+    S = cpu_pipeline(sample_tiles)
+    O, step = S["O"], S["step"]
     reps = 0
     t = time.perf_counter()
     while reps < max_reps and (reps == 0 or time.perf_counter() - t < min_seconds):
         step()
         reps += 1
     dt = (time.perf_counter() - t) / reps
-    frames = ntiles / ((WIDTH // 8) * (HEIGHT // 8))
+    frames = S["ntiles"] / TILES
     # the small configuration (a whole 256x256 quad frame, 1,024 tiles) as well
-    _, small_step, _, _ = cpu_pipeline(0, size=(256, 256))
-    small_step()
+    small = cpu_pipeline(0, size=(256, 256))
+    small["step"]()
     t = time.perf_counter()
     for _ in range(3):
-        small_step()
+        small["step"]()
     small_ms = (time.perf_counter() - t) / 3 * 1e3
-    return {"value": round(frames / dt, 5), "unit": UNIT, "cores": O.get_threads(), "kind": "port",
-            "sample": "%s of the scene through all three stages, FP64, %d rep(s); frames = tiles / 78,408" % (
-                what, reps),
-            "full_frame_ms": round(1e3 * dt / frames, 1), "small_256x256_ms": round(small_ms, 2)}
+    rec = {"value": round(frames / dt, 5), "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+           "sample": "%s of the scene through all three stages, FP64, %d rep(s); frames = tiles / 78,408" % (
+               S["what"], reps),
+           "full_frame_ms": round(1e3 * dt / frames, 1), "small_256x256_ms": round(small_ms, 2)}
+    parity = None
+    try:
+        parity = sample_parity(S)
+    except Exception as e:  # the record is informative; the GPU tests are the parity gate
+        parity = {"error": str(e).splitlines()[0][:200]}
+    return rec, parity
+
+
+def reference_kernels(S, frames=10, warmup=2):
+    """The reference's own CUDA kernels (src/TileProcessor.cuh), compiled for
+    sm_100a from the reference checkout (oracle/_ref), on the same frame:
+    convert_correct_tiles, correlate2D and generate_RBGA's kernels launched
+    back to back on the default stream (the host reads the texture-list counts
+    and window back where the reference's dynamic-parallelism driver read them
+    on the device), timed with CUDA events; also with the device synchronised
+    after every launch, as the reference's harness runs them."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refgpu
+    geom = S["geom"]
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    if not refgpu.available(geom):
+        return {"unavailable": "reference kernels for %dx%d not built (oracle/Makefile, make ref)" % (
+            geom["img_width"], geom["img_height"])}
+    dev = "cuda"
+    TX, TY, TYA = S["TX"], S["TY"], S["TYA"]
+    ptrs = lambda ts: torch.tensor([x.data_ptr() for x in ts], dtype=torch.int64, device=dev)
+    images = [torch.from_numpy(S["pitched"][c]).to(dev) for c in range(4)]
+    kernels = [torch.from_numpy(np.ascontiguousarray(S["kern"][c])).to(dev) for c in range(4)]
+    extras = [torch.from_numpy(np.ascontiguousarray(S["extra"][c])).to(dev) for c in range(4)]
+    clt = [torch.zeros(TX * TY * 768, dtype=torch.float32, device=dev) for _ in range(4)]
+    p_img, p_ker, p_ext, p_clt = ptrs(images), ptrs(kernels), ptrs(extras), ptrs(clt)
+    tasks = torch.from_numpy(np.ascontiguousarray(S["tasks"]).view(np.int32).reshape(-1, 10).copy()).to(dev)
+    n, idx = S["ntiles"], torch.from_numpy(S["corr_idx"]).to(dev)
+    stride = (2 * CORR_RADIUS + 1) ** 2
+    corrs = torch.zeros((len(S["corr_idx"]), stride), dtype=torch.float32, device=dev)
+    rstride = (TX + 1) * 8
+    rgba = torch.zeros(((TY + 1) * 8 * 4 + 8, rstride), dtype=torch.float32, device=dev)
+    lst = torch.zeros(TX * TYA + 256, dtype=torch.int32, device=dev)
+    cnt = torch.zeros(8, dtype=torch.int32, device=dev)
+    woi = torch.zeros(4, dtype=torch.int32, device=dev)
+    po = torch.from_numpy(np.ascontiguousarray(S["port_offsets"], np.float32).reshape(-1)).to(dev)
+    t = TEXTURE
+    stages = {
+        "convert": lambda: refgpu.call(geom, "ref_convert_correct_tiles", p_ext.data_ptr(), p_ker.data_ptr(),
+                                       p_img.data_ptr(), tasks.data_ptr(), p_clt.data_ptr(), S["dstride"], n, 0),
+        "correlate": lambda: refgpu.call(geom, "ref_correlate2D", p_clt.data_ptr(), 3, .25, .25, .5, FAT_ZERO,
+                                         len(S["corr_idx"]), idx.data_ptr(), stride, CORR_RADIUS, corrs.data_ptr()),
+        "texture": lambda: refgpu.call(geom, "ref_generate_RBGA", tasks.data_ptr(), n, lst.data_ptr(),
+                                       cnt.data_ptr(), woi.data_ptr(), TX, TY, p_clt.data_ptr(), po.data_ptr(),
+                                       t["colors"], t["is_lwir"], t["min_shot"], t["scale_shot"], t["diff_sigma"],
+                                       t["diff_threshold"], t["min_agree"], t["weight0"], t["weight1"],
+                                       t["weight2"], t["dust_remove"], 0, rstride, rgba.data_ptr()),
+    }
+
+    def timed(sync):
+        refgpu.call(geom, "ref_set_sync", 1 if sync else 0)
+        try:
+            for _ in range(warmup):
+                for f in stages.values():
+                    f()
+            torch.cuda.synchronize()
+            ev = {k: [] for k in stages}
+            for _ in range(frames):
+                for k, f in stages.items():
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record()
+                    f()
+                    b.record()
+                    ev[k].append((a, b))
+            torch.cuda.synchronize()
+        finally:
+            refgpu.call(geom, "ref_set_sync", 1)
+        st = {k: sum(a.elapsed_time(b) for a, b in v) / frames for k, v in ev.items()}
+        return {"ms_per_frame": round(sum(st.values()), 4), "frames_per_s": round(1e3 / sum(st.values()), 2),
+                "stages_ms": {k: round(v, 4) for k, v in st.items()}}
+
+    out = {"what": "the reference's CUDA kernels compiled for sm_100a (oracle/_ref), same frame, CUDA events, "
+                   "%d frames after %d" % (frames, warmup)}
+    out["back_to_back"] = timed(False)
+    out["synchronised_per_launch"] = timed(True)
+    return out
 
 
 def run_reference(args, rank, world, pg):
     if rank != 0:
         return None
-    O, step, ntiles, what = cpu_pipeline(args.cpu_sample_tiles)
+    # one whole frame per step: the frame the B200 arm's rank 0 runs
+    S = cpu_pipeline(0, size=(WIDTH, HEIGHT))
+    O, step = S["O"], S["step"]
     for _ in range(args.warmup):
         step()
     t = time.perf_counter()
     for _ in range(args.steps):
         step()
     dt = (time.perf_counter() - t) / args.steps
-    frames = ntiles / ((WIDTH // 8) * (HEIGHT // 8))
-    v = frames / dt
-    return {
+    v = S["ntiles"] / TILES / dt
+    out = {
         "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(1e3 / v, 3), "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": round(1e3 * dt, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded plane scene, centred PSF kernels)",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT),
-                   "sample_tiles_per_step": ntiles, "parallelism": "host threads"},
+        "config": bench_config(world),
+        "frames_per_step": 1,
         "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": O.get_threads(), "kind": "port",
-                         "sample": "%s per step through all three stages, FP64; frames = tiles / 78,408" % what},
+                         "sample": "%s per step through all three stages, FP64" % S["what"]},
         "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_kernels:
+        try:
+            out["reference_kernels"] = reference_kernels(S)
+        except Exception as e:  # beside the line, never instead of it
+            out["reference_kernels"] = {"unavailable": str(e).splitlines()[0][:200]}
+    return out
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=250)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--frames-per-step", type=int, default=FRAMES_PER_STEP,
+                    help="passes of the frame in one timed step")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample-tiles", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-kernels", action="store_true",
+                    help="reference arm: skip the rebuilt reference kernels' GPU timing")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-frame batched workload")
     ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes instead of tuned ones")
     ap.add_argument("--shapes", default="", help="fixed launch shapes, e.g. convert=8,correlate=6,textures=4")

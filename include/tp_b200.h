@@ -229,7 +229,10 @@ int tp_imclt_rbg_all(const tp_geometry *g,
  * texture_indices   : device int[tilesx * tilesya]
  * num_texture_tiles : device int[8] (inner/border count per 2x2 parity)
  * woi               : device int[4] -> {x, y, width, height} in tiles
- * Lists are in task order (the reference's order depends on atomicAdd order).
+ * Within a sub-list, entries claimed by one warp are in task order; across
+ * warps the order is the order in which their atomicAdds land (the reference's
+ * order depends on atomicAdd order too).  Tiles of one sub-list never overlap,
+ * so no output depends on the order.
  * tasks' bits 0..3 are rewritten with the N/E/S/W neighbour mask, as in the
  * reference. */
 int tp_prepare_texture_list(const tp_geometry *g,
@@ -273,10 +276,15 @@ int tp_generate_RBGA(const tp_geometry *g,
  *   - the first call on a device, with that device current, looks the
  *     array up (cudaGetSymbolAddress) once; make that first call before any
  *     stream capture;
+ *   - the address is kept with the id of the context it was found in; after
+ *     a device reset the next call looks it up again;
  *   - every call shares the array and leaves its contents behind; nothing in
- *     it needs to start at zero (each call clears the part of the list it
- *     reads and resets the counts and window); calls that overlap on the GPU
- *     race: serialise them (one stream, or events);
+ *     it needs to start at zero: each call clears the tile-marker grid over
+ *     the whole frame (not only the width x height extent, which is checked
+ *     but otherwise unused), so a call whose tasks lie inside the frame gets
+ *     the result of tp_generate_RBGA on freshly zeroed buffers, and it resets
+ *     the counts and the window; calls that overlap on the GPU race:
+ *     serialise them (one stream, or events);
  *   - tasks' bits 0..3 are rewritten with the neighbour mask, as in
  *     tp_generate_RBGA; the window of interest is not returned. */
 #define TP_NOALLOC_SCRATCH_INTS (1 << 18)

@@ -1,4 +1,5 @@
-"""Which texture outputs are well conditioned.
+"""Which texture outputs are well conditioned (checker infrastructure: used by
+the tests, smoke() and bench.py's CPU-baseline leg beside the FP64 oracle).
 
 The camera fusion of the texture stage (tile_combine_rgba) takes discrete
 choices -- best and second-best camera, worst camera for dust removal -- from
@@ -77,3 +78,47 @@ def unstable_image_mask(bad_tiles, idx, woi, TX, shape, slices):
             continue
         m[y0:y0 + 16, x0:x0 + 16] |= bad_tiles[k]
     return np.concatenate([m] * slices, axis=0)
+
+
+class _Frame:
+    """geometry and port offsets of a frame, as texture_outputs reads them"""
+
+    def __init__(self, geom, port_offsets):
+        self.geom = geom
+        self.port_offsets = port_offsets
+
+
+def unstable_tiles(oracle, geom, port_offsets, clt, tiles, keep_weights=0, colors=3, chunk=8192, trials=8):
+    """unstable_mask for the tiles `tiles` (tile numbers) of a large frame,
+    in chunks, so host memory stays bounded: each chunk's CLT is gathered into
+    compact FP64 arrays and its tiles renumbered 0..n-1 (the per-tile outputs
+    depend only on a tile's own CLT).  Returns (unstable, oracle outputs),
+    [n][ns][16][16] each, in the order of `tiles`."""
+    tiles = np.asarray(tiles, dtype=np.int64)
+    fr = _Frame(geom, port_offsets)
+    chunk = max(1, min(chunk, (geom["img_width"] // 8) * (geom["img_height"] // 8)))
+    bads, bases = [], []
+    for a in range(0, tiles.size, chunk):
+        t = tiles[a:a + chunk]
+        sub = [np.asarray(c, dtype=np.float32).reshape(-1, 768)[t].astype(np.float64).reshape(-1) for c in clt]
+        idx = ((np.arange(t.size, dtype=np.int64) << 8) | 0x80 | 0xF).astype(np.int32)
+        b, o = unstable_mask(oracle, fr, sub, idx, keep_weights, colors, trials=trials)
+        bads.append(b)
+        bases.append(o)
+    return np.concatenate(bads), np.concatenate(bases)
+
+
+def stable_errors(got, want, keep):
+    """Per-slice comparison on the stable outputs: the unstable fraction, the
+    largest error relative to the slice maximum of `want`, and the fraction of
+    stable outputs above 1e-5.  got, want, keep: [n][ns][...] arrays."""
+    out = []
+    for s in range(want.shape[1]):
+        g = np.asarray(got[:, s], np.float64)
+        w = np.asarray(want[:, s], np.float64)
+        k = keep[:, s]
+        den = np.abs(w).max() or 1.0
+        e = np.abs(g - w)[k] / den
+        out.append({"unstable": float(1.0 - k.mean()), "max": float(e.max()) if e.size else 0.0,
+                    "frac_gt_1e-5": float((e > TOL).mean()) if e.size else 0.0})
+    return out

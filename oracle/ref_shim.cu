@@ -38,7 +38,24 @@
         }                                                                           \
     } while (0)
 
+/* 1: synchronise the device after every launch, as the reference's harness
+ * does (src/dtt8x8.cu:574-575); 0: launch back to back on the default stream
+ * (the host copies that read the list counts and the window still wait), for
+ * timing the kernels themselves. */
+static int g_sync = 1;
+
+#define SYNC_AFTER_LAUNCH()                          \
+    do {                                             \
+        if (g_sync) RET_CUDA(cudaDeviceSynchronize()); \
+    } while (0)
+
 extern "C" {
+
+int ref_set_sync(int on)
+{
+    g_sync = on ? 1 : 0;
+    return 0;
+}
 
 int ref_tilesx(void) { return TILESX; }
 int ref_tilesy(void) { return TILESY; }
@@ -54,7 +71,7 @@ int ref_convert_correct_tiles(float **gpu_kernel_offsets, float **gpu_kernels, f
     convert_correct_tiles<<<grid, threads>>>(gpu_kernel_offsets, gpu_kernels, gpu_images, gpu_tasks,
                                              gpu_clt, dstride, num_tiles, lpf_mask);
     RET_CUDA(cudaGetLastError());
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     return 0;
 }
 
@@ -68,7 +85,7 @@ int ref_correlate2D(float **gpu_clt, int colors, float scale0, float scale1, flo
                                    num_corr_tiles, gpu_corr_indices, corr_stride, corr_radius,
                                    gpu_corrs);
     RET_CUDA(cudaGetLastError());
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     return 0;
 }
 
@@ -89,7 +106,7 @@ int ref_textures_accumulate(int *woi, float **gpu_clt, size_t num_texture_tiles,
                                            weight2, dust_remove, keep_weights, texture_rbg_stride,
                                            gpu_texture_rbg, texture_stride, gpu_texture_tiles);
     RET_CUDA(cudaGetLastError());
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     return 0;
 }
 
@@ -103,7 +120,7 @@ int ref_imclt_rbg(float *gpu_clt, float *gpu_rbg, int color, int v_offset, int h
     dim3 grid((tiles_in_pass + IMCLT_TILES_PER_BLOCK - 1) / IMCLT_TILES_PER_BLOCK, 1, 1);
     imclt_rbg<<<grid, threads>>>(gpu_clt, gpu_rbg, color, v_offset, h_offset, dstride);
     RET_CUDA(cudaGetLastError());
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     return 0;
 }
 
@@ -117,14 +134,14 @@ int ref_prepare_texture_list(struct tp_task *gpu_tasks, int num_tiles, int *gpu_
     dim3 blocks0((width + nthr - 1) >> THREADS_DYNAMIC_BITS, height, 1);
     clear_texture_list<<<blocks0, threads0>>>(gpu_texture_indices, width, height);
     RET_CUDA(cudaGetLastError());
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     dim3 threads(nthr, 1, 1);
     dim3 blocks((num_tiles + nthr - 1) >> THREADS_DYNAMIC_BITS, 1, 1);
     if (blocks.x) {
         mark_texture_tiles<<<blocks, threads>>>(gpu_tasks, num_tiles, gpu_texture_indices);
         RET_CUDA(cudaGetLastError());
     }
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     int woi0[4] = {TILESX, TILESY, 0, 0};
     RET_CUDA(cudaMemcpy(gpu_woi, woi0, sizeof(woi0), cudaMemcpyHostToDevice));
     if (blocks.x) {
@@ -132,14 +149,14 @@ int ref_prepare_texture_list(struct tp_task *gpu_tasks, int num_tiles, int *gpu_
                                                          gpu_woi);
         RET_CUDA(cudaGetLastError());
     }
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     RET_CUDA(cudaMemset(gpu_num_texture_tiles, 0, 8 * sizeof(int)));
     if (blocks.x) {
         gen_texture_list<<<blocks, threads>>>(gpu_tasks, num_tiles, gpu_texture_indices,
                                               gpu_num_texture_tiles, gpu_woi);
         RET_CUDA(cudaGetLastError());
     }
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     int woi[4];
     RET_CUDA(cudaMemcpy(woi, gpu_woi, sizeof(woi), cudaMemcpyDeviceToHost));
     woi[2] += 1 - woi[0];
@@ -175,7 +192,7 @@ int ref_generate_RBGA(struct tp_task *gpu_tasks, int num_tiles, int *gpu_texture
     clear_texture_rbga<<<blocks2, threads2>>>(texture_width, texture_tiles_height * texture_slices,
                                               texture_rbga_stride, gpu_texture_tiles);
     RET_CUDA(cudaGetLastError());
-    RET_CUDA(cudaDeviceSynchronize());
+    SYNC_AFTER_LAUNCH();
     for (int pass = 0; pass < 8; pass++) {
         dim3 threads_texture(TEXTURE_THREADS_PER_TILE, NUM_CAMS, 1);
         int border_tile = pass >> 2;
@@ -189,7 +206,7 @@ int ref_generate_RBGA(struct tp_task *gpu_tasks, int num_tiles, int *gpu_texture
             is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold, min_agree, weight0, weight1,
             weight2, dust_remove, 0, texture_rbga_stride, gpu_texture_tiles, 0, gpu_texture_tiles);
         RET_CUDA(cudaGetLastError());
-        RET_CUDA(cudaDeviceSynchronize());
+        SYNC_AFTER_LAUNCH();
     }
     return 0;
 }

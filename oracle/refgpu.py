@@ -21,7 +21,7 @@ SIGS = {
     "ref_imclt_rbg": [_P, _P, _I, _I, _I, _S],
     "ref_prepare_texture_list": [_P, _I, _P, _P, _P, _I, _I],
     "ref_generate_RBGA": [_P, _I, _P, _P, _P, _I, _I, _P, _P, _I, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, _I, _S, _P],
-    "ref_tilesx": [], "ref_tilesy": [], "ref_tilesya": [],
+    "ref_tilesx": [], "ref_tilesy": [], "ref_tilesya": [], "ref_set_sync": [_I],
 }
 
 

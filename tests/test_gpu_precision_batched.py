@@ -56,6 +56,29 @@ def test_stage_errors_against_fp64(oracle, name, peak):
 SIZES = [(320, 240), (640, 480), (256, 256), (800, 600), (512, 384), (1024, 768)]
 
 
+def _check_rgba(oracle, geom, tasks, TX, TY, clt, port_offsets, rgba, woi, what):
+    """The overlapped RGBA image of one frame against the FP64 oracle's on the
+    same CLT, on pixels all of whose tiles are stable (as in the small-frame
+    parity tests); returns the per-slice record."""
+    import conditioning
+    from test_gpu_parity import assert_close_on
+    stride = rgba.shape[1]
+    o, _, _, _, woi_o = oracle.generate_RBGA(geom, tasks, TX, TY, clt, port_offsets, stride, rgba.shape[0] + 8)
+    assert np.array_equal(woi, woi_o), what
+    h, w = (woi[3] + 1) * 8, (woi[2] + 1) * 8
+    txy = tasks["txy"].astype(np.int64)
+    textured = (tasks["task"] & 0xF) != 0
+    tiles = ((txy & 0xFFFF) + (txy >> 16) * TX)[textured]
+    bad, _ = conditioning.unstable_tiles(oracle, geom, port_offsets, clt, tiles)
+    codes = (tiles << 8).astype(np.int64)
+    m = conditioning.unstable_image_mask(bad.any(axis=1), codes, woi, TX, (h, w), 4)
+    assert m.mean() <= 0.01, (what, m.mean())
+    b, r = rgba[:4 * h, :w], o[:4 * h, :w]
+    assert_close_on(b, r, ~m, 1e-5, 4e-4)
+    sl = lambda a: a.reshape(4, h, w)[None]
+    return conditioning.stable_errors(sl(b), sl(r), sl(~m))
+
+
 def _batch():
     rng = np.random.default_rng(77)
     cases = []
@@ -102,6 +125,8 @@ def test_batched_uneven_sparse_frames(oracle):
         co = oracle.correlate2D(c.geom, [x.astype(np.float64) for x in clt], 3, .25, .25, .5, 0.05, c.corr_idx,
                                 225, 7)
         assert rel_err(o["corrs"].cpu().numpy(), co) < 1e-5, (c.W, c.H)
+        _check_rgba(oracle, c.geom, c.tasks, c.TX, c.TY, clt, c.port_offsets, o["rgba"].cpu().numpy(),
+                    o["woi"].cpu().numpy(), (c.W, c.H))
     eager = [(o["corrs"].clone(), o["rgba"].clone()) for o in outs]
     # the whole batch as one CUDA graph (the calls' first use on this device is above)
     side = torch.cuda.Stream()
@@ -130,3 +155,50 @@ def test_batched_uneven_sparse_frames(oracle):
     print("\nbatch of %d uneven sparse frames: %.3f ms per batch, %.1f frames/s" % (len(cases), ms,
                                                                                     len(cases) / ms * 1e3))
     del g
+
+
+def test_bench_batched_frames_vs_oracle(native, oracle):
+    """Four of the bench's own 64 batched frames -- the smallest, the largest,
+    the sparsest and the densest -- run through the three calls on the
+    bench's shared buffers, each checked against the FP64 oracle: CLT and
+    correlations within 1e-5, the overlapped RGBA image on stable pixels."""
+    import os
+    import sys
+    import torch
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    pipe = bench.FramePipeline(seed=100, device="cuda:0")
+    batch = bench.BatchedFrames(pipe, n=64, seed=11)
+    fs = batch.frames
+    area = [f["size"][0] * f["size"][1] for f in fs]
+    act = [f["activity"] for f in fs]
+    pick = sorted({int(np.argmin(area)), int(np.argmax(area)), int(np.argmin(act)), int(np.argmax(act))})
+    records = {}
+    for k in pick:
+        f = fs[k]
+        batch.run_frame(f)
+        torch.cuda.synchronize()
+        geom, TX, TY = f["geom"], f["TX"], f["TY"]
+        n = TX * TY * 768
+        clt = [pipe.clt[c][:n].cpu().numpy() for c in range(4)]
+        images = np.stack([x.cpu().numpy() for x in f["images"]])
+        kernels = [x.cpu().numpy() for x in f["kernels"]]
+        extras = [x.cpu().numpy() for x in f["extras"]]
+        want = oracle.convert_correct_tiles(geom, extras, kernels, images, f["dstride"], f["tasks_np"])
+        what = "frame %d %dx%d activity %.2f" % (k, f["size"][0], f["size"][1], f["activity"])
+        e_clt = max(rel_err(clt[c], want[c]) for c in range(4))
+        assert e_clt < 1e-5, (what, e_clt)
+        idx = f["corr_idx"].cpu().numpy()
+        co = oracle.correlate2D(geom, [x.astype(np.float64) for x in clt], 3, .25, .25, .5, bench.FAT_ZERO, idx,
+                                pipe.corr_stride, bench.CORR_RADIUS)
+        cb = pipe.corrs[:len(idx)].cpu().numpy()
+        e_corr = rel_err(cb[:, :225], co[:, :225])
+        assert e_corr < 1e-5, (what, e_corr)
+        st = f["rgba_stride"]
+        rows = (TY + 1) * 8 * 4
+        rgba = pipe.rgba.view(-1)[:rows * st].view(rows, st).cpu().numpy()
+        rec = _check_rgba(oracle, geom, f["tasks_np"], TX, TY, clt, pipe.port_offsets.cpu().numpy(), rgba,
+                          pipe.woi.cpu().numpy(), what)
+        records[what] = {"clt_max": e_clt, "corr_max": e_corr, "rgba": rec}
+    print("\nbench batched frames vs the FP64 oracle " + json.dumps(records))

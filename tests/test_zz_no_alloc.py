@@ -63,3 +63,59 @@ def test_noalloc_matches_generate_rbga(native, name):
         assert np.array_equal(got[touched], want[touched]), k
         assert np.all(got[~touched] == 5.0 + k)
         assert np.array_equal(api.tasks_from_device(t2)["task"], tasks_after["task"])
+
+
+@pytest.mark.parametrize("k", [1, 3])
+def test_noalloc_smaller_extent_after_full_frame(native, k):
+    """A full-frame call leaves tile markers in every row of the shared array;
+    the next call declares a list extent k rows shorter (height = tilesy - k)
+    and has textured tiles in row height - 1, whose south neighbour is row
+    `height`.  Its task bits and RGBA image must be those of tp_generate_RBGA
+    run with the same extent on freshly zeroed buffers, where that row holds
+    no marker."""
+    import torch
+    import gpu_runner as R
+    from tile_processor_gpu_b200 import api
+    full = Case(256, 256, seed=12, border_mode=0)
+    rows_kept = np.zeros((full.TY, full.TX), dtype=bool)
+    height = full.TY - k
+    rows_kept[:height] = True
+    short = Case(256, 256, seed=12, border_mode=0, mask=rows_kept)
+    assert np.any((short.tasks["txy"] >> 16) == height - 1)
+    p = TEX
+    args = (p["colors"], p["is_lwir"], p["min_shot"], p["scale_shot"], p["diff_sigma"], p["diff_threshold"],
+            p["min_agree"], p["weight0"], p["weight1"], p["weight2"], p["dust_remove"], p["keep_weights"])
+    stride = (full.TX + 1) * 8 + 40
+    rows = (full.TY + 1) * 8 * 4
+    fr_full = R.Frame(full)
+    R.convert(fr_full)
+    fr = R.Frame(short)
+    R.convert(fr)
+    # the drop-in on freshly zeroed buffers, extent width x height
+    want_out = torch.full((rows + 8, stride), 3.0, device="cuda")
+    t_ref = api.tasks_to_device(short.tasks, "cuda")
+    idx = torch.zeros(short.TX * short.TYA + 256, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(8, dtype=torch.int32, device="cuda")
+    woi = torch.zeros(4, dtype=torch.int32, device="cuda")
+    api.generate_RBGA(fr.g, t_ref, short.num_tiles, idx, cnt, woi, short.TX, height, fr.p_clt, fr.port_offsets,
+                      *args, stride, want_out)
+    torch.cuda.synchronize()
+    want = want_out.cpu().numpy()
+    want_tasks = api.tasks_from_device(t_ref)["task"]
+    # a full frame through the no-alloc call first: its markers fill every row
+    dirty = torch.zeros((rows + 8, stride), device="cuda")
+    t_full = api.tasks_to_device(full.tasks, "cuda")
+    api.generate_RBGA_noalloc(fr_full.g, t_full, full.num_tiles, full.TX, full.TY, fr_full.p_clt,
+                              fr_full.port_offsets, *args, stride, dirty)
+    # then the shorter extent, twice in a row
+    for rep in range(2):
+        out = torch.full((rows + 8, stride), 5.0 + rep, device="cuda")
+        t2 = api.tasks_to_device(short.tasks, "cuda")
+        api.generate_RBGA_noalloc(fr.g, t2, short.num_tiles, short.TX, height, fr.p_clt, fr.port_offsets, *args,
+                                  stride, out)
+        torch.cuda.synchronize()
+        assert np.array_equal(api.tasks_from_device(t2)["task"], want_tasks), rep
+        got = out.cpu().numpy()
+        touched = want != 3.0
+        assert np.array_equal(got[touched], want[touched]), rep
+        assert np.all(got[~touched] == 5.0 + rep)

@@ -137,12 +137,45 @@ int texture_smem_setup()
 }
 
 /* Scratch of tp_generate_RBGA_noalloc: [0, 8) sub-list counts, [8, 12) window
- * of interest, [16, ...) the texture list.  Needs no initial contents. */
+ * of interest, [16, ...) the texture list and its tile-marker grid.  Needs no
+ * initial contents: every call clears the whole marker grid it reads. */
 static __device__ __align__(256) int g_rbga_scratch[TP_NOALLOC_SCRATCH_INTS];
 
-/* per-device address of g_rbga_scratch, looked up on first use */
+/* Per-device address of g_rbga_scratch, looked up on the first call on that
+ * device, together with the unique id of the context it belongs to.  A
+ * device reset destroys the primary context and the module with it; the next
+ * call then sees a new context id and looks the array up again instead of
+ * handing the kernels an address of the old context. */
 std::mutex g_scratch_mutex;
 int *g_scratch_ptr[128];
+unsigned long long g_scratch_ctx[128];
+typedef CUresult (*PFN_ctx_get_current)(CUcontext *);
+typedef CUresult (*PFN_ctx_get_id)(CUcontext, unsigned long long *);
+
+/* unique id of the calling thread's current context (0 when unavailable) */
+unsigned long long current_context_id()
+{
+    static PFN_ctx_get_current get_current = nullptr;
+    static PFN_ctx_get_id get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PFN_ctx_get_current>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PFN_ctx_get_id>(p);
+        looked_up = true;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 
 int noalloc_scratch(int **out)
 {
@@ -151,11 +184,15 @@ int noalloc_scratch(int **out)
     if (e != cudaSuccess) return fail(TP_ERR_NO_DEVICE, "cudaGetDevice: %s", cudaGetErrorString(e));
     if (dev < 0 || dev >= 128) return fail(TP_ERR_NO_DEVICE, "device %d", dev);
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
+    /* 0 when this thread has no current context yet: the lookup below makes
+     * the device's primary context current, and its id is read after it */
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_ptr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_rbga_scratch);
         if (e != cudaSuccess) return fail(TP_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
         g_scratch_ptr[dev] = static_cast<int *>(p);
+        g_scratch_ctx[dev] = current_context_id();
     }
     *out = g_scratch_ptr[dev];
     return TP_OK;
@@ -483,10 +520,13 @@ static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, in
     if ((rc = texture_smem_setup())) return rc;
     /* The RGBA clear and the four passes continue prepare_list's chain of
      * programmatic dependents.  The clear waits on entry for the list's last
-     * kernel.  A pass prefetches its first tile's CLT and reads the list before it
-     * waits for the launch before it (the clear, or the previous pass, which
-     * read-modify-writes the RGBA image): that launch released it only after
-     * its own wait, so the list was complete by then. */
+     * kernel and releases its dependent only after that wait.  A pass releases
+     * its own dependent on entry, then prefetches its first tile's CLT and
+     * reads the list, and only then waits for the launch before it (the
+     * clear, or the previous pass, which read-modify-writes the RGBA image).
+     * So a pass can start only after every earlier pass has started, and the
+     * first pass only after the clear released it, which the clear did once
+     * the list was complete: every pass reads a finished list. */
     {
         const int max_rows = (gd.TY + 1) * 8 * (colors + 1);
         const cudaError_t err = launch_chained(true, grid_for(max_rows, 1, sms, 16), 256, 0, s, tp::k_clear_rbga,
@@ -606,11 +646,23 @@ int tp_generate_RBGA_noalloc(const tp_geometry *g, tp_task *tasks, int num_tiles
     if (rc) return rc;
     const long long need = (long long)gd.TX * gd.TYA + 16;
     if (need > TP_NOALLOC_SCRATCH_INTS)
-        return fail(TP_ERR_ARG, "frame needs %lld scratch ints, the library holds %d (%d x %d tiles max)", need,
-                    TP_NOALLOC_SCRATCH_INTS, gd.TX, (TP_NOALLOC_SCRATCH_INTS - 16) / (gd.TX > 0 ? gd.TX : 1));
+        return fail(TP_ERR_ARG, "frame needs %lld scratch ints, the library holds %d (%d tiles across: at most %d "
+                    "tile rows)", need, TP_NOALLOC_SCRATCH_INTS, gd.TX,
+                    ((TP_NOALLOC_SCRATCH_INTS - 16) / (gd.TX > 0 ? gd.TX : 1)) & ~3);
+    if (width < 0 || height < 0 || width > gd.TX || height > gd.TY)
+        return fail(TP_ERR_ARG, "list extent %dx%d outside %dx%d tiles", width, height, gd.TX, gd.TY);
     int *scratch = nullptr;
     if ((rc = noalloc_scratch(&scratch))) return rc;
-    return tp_generate_RBGA(g, tasks, num_tiles, scratch + 16, scratch, scratch + 8, width, height, clt,
+    /* The list kernels read the marker of every neighbour of every texture
+     * tile, wherever it lies; caller buffers hold zeros there where the
+     * caller's width x height extent leaves them uncleared, but the shared
+     * array holds whatever an earlier call left.  So the marker grid is
+     * cleared over the whole frame (tilesx + 1 columns, tilesy rows), which
+     * gives the result of tp_generate_RBGA on freshly zeroed buffers for any
+     * extent the caller passes. */
+    (void)width;
+    (void)height;
+    return tp_generate_RBGA(g, tasks, num_tiles, scratch + 16, scratch, scratch + 8, gd.TX, gd.TY, clt,
                             port_offsets, colors, is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold,
                             min_agree, weight0, weight1, weight2, dust_remove, keep_weights, texture_rbga_stride,
                             texture_tiles, stream);
