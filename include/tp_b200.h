@@ -21,7 +21,9 @@
  * Every call validates its host-visible arguments and returns TP_OK or a
  * negative TP_ERR_* code (the reference kernels return void and silently skip
  * bad input); tp_last_error() gives a one-line reason.  No call allocates
- * device memory, synchronises the device or reads device data on the host.
+ * device memory, and none synchronises the device or reads device data on the
+ * host, except the first tensor-core call on a device (it copies the
+ * transform tables) and tp_tc_status, which say so.
  * Device-side inputs that the host cannot see (task records, index lists) are
  * range-checked in the kernels: an out-of-range entry is skipped instead of
  * being read or written out of bounds.
@@ -450,6 +452,99 @@ int tp_mlp_combine(size_t n, const float *plain, const float *out, float gate, f
 /* Adam step `step` (1, 2, ...) on n parameters */
 int tp_mlp_adam(size_t n, float *param, const float *grad, float *m, float *v, float lr, float beta1, float beta2,
                 float eps, int step, tp_stream_t stream);
+
+/* ---- tensor-core precision forms of the stages ----------------------------------
+ * The same calls as above, with each stage's batched 8x8 transforms (the
+ * DCT-IV / DST-IV / DCT-II / DST-II pairs of src/dtt8x8.cuh:382-463,
+ * :621-745 on every quadrant) run as tcgen05 GEMMs: 64 x 64 matrices per
+ * quadrant, operands split into two 16-bit halves (hi + lo), three MMAs per
+ * product, FP32 accumulation in tensor memory.  The element-wise steps (CLT
+ * products, normalisation, LPFs, unfolds) are the plain path's.  `format`:
+ *   TP_TC_FP16X2  FP16 halves (22 significant bits; rows scaled by a power of
+ *                 two to stay in FP16 range)
+ *   TP_TC_BF16X2  BF16 halves (16 significant bits, no scaling)
+ * The first call on a device copies the transform tables to it (synchronous;
+ * make it before any stream capture).  A bounded wait inside a kernel that
+ * runs out leaves that kernel's outputs incomplete and is reported by
+ * tp_tc_status. */
+#define TP_TC_FP16X2 0
+#define TP_TC_BF16X2 1
+/* convert_correct_tiles (src/TileProcessor.cuh:1859-1937), same arguments:
+ * the 2-D DCT-IV (and for green the DST-IV x DCT-IV) of each folded tile on
+ * the tensor cores; fold, kernel convolution, shifts and LPF as the plain
+ * path */
+int tp_convert_correct_tiles_tc(const tp_geometry *g,
+                                float *const *kernel_offsets,
+                                float *const *kernels,
+                                float *const *images,
+                                const tp_task *tasks,
+                                float *const *clt,
+                                size_t dstride,
+                                int num_tiles,
+                                int lpf_mask,
+                                int format,
+                                tp_stream_t stream);
+/* correlate2D (src/TileProcessor.cuh:1176-1443), same arguments */
+int tp_correlate2D_tc(const tp_geometry *g,
+                      float *const *clt,
+                      int colors,
+                      float scale0, float scale1, float scale2,
+                      float fat_zero,
+                      size_t num_corr_tiles,
+                      const int *corr_indices,
+                      size_t corr_stride,
+                      int corr_radius,
+                      float *corrs,
+                      int format,
+                      tp_stream_t stream);
+/* textures_accumulate (src/TileProcessor.cuh:2207-2579) and generate_RBGA
+ * (:1446-1615), same arguments, plus tile_scratch: a device array [4] of
+ * per-camera buffers of the CLT's size and layout ([tilesy * tilesx][3][256]
+ * floats) that receive each listed job's inverse CLT, computed on the tensor
+ * cores, before the debayer and camera fusion read it. */
+int tp_textures_accumulate_tc(const tp_geometry *g,
+                              const int *woi,
+                              float *const *clt,
+                              size_t num_texture_tiles,
+                              const int *texture_indices,
+                              const float *port_offsets,
+                              int colors, int is_lwir,
+                              float min_shot, float scale_shot,
+                              float diff_sigma, float diff_threshold,
+                              float min_agree,
+                              float weight0, float weight1, float weight2,
+                              int dust_remove, int keep_weights,
+                              size_t texture_rbg_stride, float *texture_rbg,
+                              size_t texture_stride, float *texture_tiles,
+                              float *const *tile_scratch,
+                              int format,
+                              tp_stream_t stream);
+int tp_generate_RBGA_tc(const tp_geometry *g,
+                        tp_task *tasks, int num_tiles,
+                        int *texture_indices, int *num_texture_tiles,
+                        int *woi, int width, int height,
+                        float *const *clt,
+                        const float *port_offsets,
+                        int colors, int is_lwir,
+                        float min_shot, float scale_shot,
+                        float diff_sigma, float diff_threshold,
+                        float min_agree,
+                        float weight0, float weight1, float weight2,
+                        int dust_remove, int keep_weights,
+                        size_t texture_rbga_stride, float *texture_tiles,
+                        float *const *tile_scratch,
+                        int format,
+                        tp_stream_t stream);
+/* *timed_out = 1 when a tensor-core stage kernel's wait ran out since the
+ * last clear (synchronous); clear != 0 resets it.  No counterpart in the
+ * reference. */
+int tp_tc_status(int *timed_out, int clear);
+/* The 64 KB shared-memory image of a stage's split transform matrices
+ * (stage 0 correlation, 1 inverse CLT, 2 forward CLT): uint16 halves, the
+ * four hi quadrants then the four lo, each 64 rows x 64 K, 128-byte
+ * swizzled.  Host only (no device needed); for checking and inspection.  No
+ * counterpart in the reference. */
+int tp_tc_table_image(int format, int stage, void *out);
 
 #ifdef __cplusplus
 }

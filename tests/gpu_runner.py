@@ -27,12 +27,23 @@ class Frame:
         self.p_clt = api.PointerArray(self.clt)
         self.port_offsets = torch.from_numpy(case.port_offsets.reshape(-1)).to(device)
 
+    def tile_scratch(self):
+        """per-camera tile buffers of the CLT's size (the tensor-core texture path)"""
+        if not hasattr(self, "_tiles"):
+            self._tiles = [torch.zeros_like(c) for c in self.clt]
+            self.p_tiles = api.PointerArray(self._tiles)
+        return self.p_tiles
+
     def clt_numpy(self):
         return [c.cpu().numpy() for c in self.clt]
 
     def set_clt(self, clt):
         for c in range(4):
             self.clt[c].copy_(torch.from_numpy(np.asarray(clt[c], dtype=np.float32)))
+
+
+def _tc_fmt(impl):
+    return api.TC_FP16X2 if impl == "tc_fp16" else api.TC_BF16X2
 
 
 def convert(fr, lpf_mask=0, impl="b200", num_tiles=None):
@@ -43,6 +54,9 @@ def convert(fr, lpf_mask=0, impl="b200", num_tiles=None):
     if impl == "b200":
         api.convert_correct_tiles(fr.g, fr.p_extra, fr.p_kernels, fr.p_images, fr.tasks, fr.p_clt, c.dstride, n,
                                   lpf_mask)
+    elif impl.startswith("tc_"):
+        api.convert_correct_tiles_tc(fr.g, fr.p_extra, fr.p_kernels, fr.p_images, fr.tasks, fr.p_clt, c.dstride, n,
+                                     lpf_mask, fmt=_tc_fmt(impl))
     else:
         refgpu.call(c.geom, "ref_convert_correct_tiles", fr.p_extra.dev.data_ptr(), fr.p_kernels.dev.data_ptr(),
                     fr.p_images.dev.data_ptr(), fr.tasks.data_ptr(), fr.p_clt.dev.data_ptr(), c.dstride, n, lpf_mask)
@@ -57,6 +71,9 @@ def correlate(fr, idx, colors=3, scales=(0.25, 0.25, 0.5), fat_zero=0.05, radius
     out = torch.full((max(len(idx), 1), stride), -7.0, dtype=torch.float32, device=DEV)
     if impl == "b200":
         api.correlate2D(fr.g, fr.p_clt, colors, *scales, fat_zero, len(idx), idx_d, stride, radius, out)
+    elif impl in ("tc_fp16", "tc_bf16"):
+        api.correlate2D_tc(fr.g, fr.p_clt, colors, *scales, fat_zero, len(idx), idx_d, stride, radius, out,
+                           fmt=api.TC_FP16X2 if impl == "tc_fp16" else api.TC_BF16X2)
     else:
         refgpu.call(c.geom, "ref_correlate2D", fr.p_clt.dev.data_ptr(), colors, *scales, fat_zero, len(idx),
                     idx_d.data_ptr(), stride, radius, out.data_ptr())
@@ -78,6 +95,9 @@ def textures_tiles(fr, idx, keep_weights=0, impl="b200", **kw):
             p["min_agree"], p["weight0"], p["weight1"], p["weight2"], p["dust_remove"], keep_weights)
     if impl == "b200":
         api.textures_accumulate(fr.g, None, fr.p_clt, len(idx), idx_d, fr.port_offsets, *args, 0, None, stride, out)
+    elif impl.startswith("tc_"):
+        api.textures_accumulate_tc(fr.g, None, fr.p_clt, len(idx), idx_d, fr.port_offsets, *args, 0, None, stride,
+                                   out, fr.tile_scratch(), fmt=_tc_fmt(impl))
     else:
         refgpu.call(fr.case.geom, "ref_textures_accumulate", None, fr.p_clt.dev.data_ptr(), len(idx),
                     idx_d.data_ptr(), fr.port_offsets.data_ptr(), *args, 0, None, stride, out.data_ptr())
@@ -132,6 +152,9 @@ def rgba(fr, impl="b200", **kw):
     if impl == "b200":
         api.generate_RBGA(fr.g, tasks, c.num_tiles, idx, counts, woi, c.TX, c.TY, fr.p_clt, fr.port_offsets,
                           *args, stride, out)
+    elif impl.startswith("tc_"):
+        api.generate_RBGA_tc(fr.g, tasks, c.num_tiles, idx, counts, woi, c.TX, c.TY, fr.p_clt, fr.port_offsets,
+                             *args, stride, out, fr.tile_scratch(), fmt=_tc_fmt(impl))
     else:
         refgpu.call(c.geom, "ref_generate_RBGA", tasks.data_ptr(), c.num_tiles, idx.data_ptr(), counts.data_ptr(),
                     woi.data_ptr(), c.TX, c.TY, fr.p_clt.dev.data_ptr(), fr.port_offsets.data_ptr(), *args, stride,

@@ -1,0 +1,194 @@
+"""The tensor-core precision forms of the stages (split FP16 / BF16 operands,
+FP32 accumulation) against the FP64 oracle and the plain FP32 path, through
+the C ABI.
+
+Bounds, relative to the oracle's largest magnitude: FP16 halves (22
+significant bits) within 1e-5 like the plain path, BF16 halves (16 bits)
+within 1e-4.  Every call also leaves the kernels' bounded-wait status clear.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from cases import Case, rel_err, rms_err
+
+pytestmark = pytest.mark.gpu
+
+BOUND = {"tc_fp16": 1e-5, "tc_bf16": 1e-4}
+
+
+@pytest.fixture(scope="module")
+def frames(native):
+    import gpu_runner as R
+    out = {}
+    for name, kw in {"A256": dict(width=256, height=256, seed=1),
+                     "hdr512": dict(width=512, height=384, seed=6, scene="plane", peak=1e4),
+                     "odd320": dict(width=320, height=240, seed=3, border_mode=1)}.items():
+        fr = R.Frame(Case(**kw))
+        clt = R.convert(fr)
+        out[name] = (fr, clt)
+    return out
+
+
+@pytest.mark.parametrize("impl", ["tc_fp16", "tc_bf16"])
+@pytest.mark.parametrize("name", ["A256", "hdr512", "odd320"])
+def test_correlate2D_tc(frames, oracle, impl, name):
+    import gpu_runner as R
+    from tile_processor_gpu_b200 import api
+    fr, clt = frames[name]
+    c = fr.case
+    fr.set_clt(clt)
+    c64 = [x.astype(np.float64) for x in clt]
+    want = oracle.correlate2D(c.geom, c64, 3, .25, .25, .5, 0.05, c.corr_idx, 228, 7)
+    got = R.correlate(fr, c.corr_idx, impl=impl)
+    plain = R.correlate(fr, c.corr_idx)
+    e = {"max": rel_err(got[:, :225], want[:, :225]), "rms": rms_err(got[:, :225], want[:, :225]),
+         "plain_max": rel_err(plain[:, :225], want[:, :225])}
+    print("\ncorrelate2D %s %s %s" % (impl, name, json.dumps({k: float("%.3g" % v) for k, v in e.items()})))
+    assert api.tc_status() == 0
+    assert e["max"] < BOUND[impl], e
+    # the stride padding is left alone, as by the plain path
+    assert np.all(got[:, 225:] == -7.0)
+
+
+@pytest.mark.parametrize("impl", ["tc_fp16", "tc_bf16"])
+def test_correlate2D_tc_radius_mono_ragged(frames, oracle, impl):
+    """radius 4, one colour, and an index list whose length is not a multiple
+    of the 128-entry block (with out-of-range entries skipped)"""
+    import gpu_runner as R
+    from tile_processor_gpu_b200 import api
+    fr, clt = frames["A256"]
+    c = fr.case
+    fr.set_clt(clt)
+    idx = c.corr_idx[:1000].copy()
+    idx[7] = (c.TX * c.TY + 5) << 8       # tile out of range: skipped
+    idx[9] = (3 << 8) | 6                 # pair 6: skipped
+    c64 = [x.astype(np.float64) for x in clt]
+    keep = np.ones(len(idx), bool)
+    keep[[7, 9]] = False
+    for colors, r in ((3, 4), (1, 7)):
+        sz = (2 * r + 1) ** 2
+        want = oracle.correlate2D(c.geom, c64, colors, .25, .25, .5, 0.05, idx[keep], sz + 3, r)
+        got = R.correlate(fr, idx, colors=colors, radius=r, impl=impl)
+        assert rel_err(got[keep, :sz], want[:, :sz]) < BOUND[impl], (colors, r)
+        assert np.all(got[~keep] == -7.0)
+    assert api.tc_status() == 0
+
+
+@pytest.mark.parametrize("impl", ["tc_fp16", "tc_bf16"])
+@pytest.mark.parametrize("name", ["A256", "hdr512", "odd320"])
+def test_convert_tc(frames, oracle, impl, name):
+    import gpu_runner as R
+    from tile_processor_gpu_b200 import api
+    fr, clt = frames[name]
+    c = fr.case
+    try:
+        for lpf_mask in (0, 7):
+            got = R.convert(fr, impl=impl, lpf_mask=lpf_mask)
+            want = oracle.convert_correct_tiles(c.geom, c.extra, c.kernels, c.pitched, c.dstride, c.tasks,
+                                                lpf_mask=lpf_mask)
+            e = max(rel_err(got[k], want[k]) for k in range(4))
+            r = max(rms_err(got[k], want[k]) for k in range(4))
+            print("\nconvert_correct_tiles %s %s lpf_mask %d: max %.3g rms %.3g" % (impl, name, lpf_mask, e, r))
+            assert e < BOUND[impl], (lpf_mask, e)
+    finally:
+        fr.set_clt(clt)
+    assert api.tc_status() == 0
+
+
+def _stable_check(got, want, keep, bound, frac=1e-4, hard=1e-3):
+    """|got - want| <= bound * slice max on the stable outputs, except a
+    fraction `frac` of them (near-tie pixels the probe did not flip), which
+    stay within `hard`"""
+    import conditioning
+    rec = conditioning.stable_errors(got, want, keep)
+    for s, r in enumerate(rec):
+        b = np.asarray(got[:, s], np.float64)[keep[:, s]]
+        w = np.asarray(want[:, s], np.float64)[keep[:, s]]
+        den = np.abs(w).max() or 1.0
+        err = np.abs(b - w) / den
+        assert float((err > bound).mean()) <= frac, (s, r)
+        assert err.max() < hard, (s, r)
+    return rec
+
+
+@pytest.mark.parametrize("impl", ["tc_fp16", "tc_bf16"])
+@pytest.mark.parametrize("name,colors", [("A256", 3), ("hdr512", 3), ("A256", 1)])
+def test_textures_tc(frames, oracle, impl, name, colors):
+    """texture tiles (keep_weights = 1: colour, alpha, port weights, rms)
+    against the oracle on stable outputs; colour and alpha within the bound,
+    weights and rms within 10x it"""
+    import conditioning
+    import gpu_runner as R
+    from tile_processor_gpu_b200 import api
+    fr, clt = frames[name]
+    c = fr.case
+    fr.set_clt(clt)
+    c64 = [x.astype(np.float64) for x in clt]
+    got = R.textures_tiles(fr, c.tex_idx, keep_weights=1, impl=impl, colors=colors)
+    bad, want = conditioning.unstable_mask(oracle, c, c64, c.tex_idx, 1, colors=colors)
+    ncol = colors
+    rec = _stable_check(got[:, :ncol + 1], want[:, :ncol + 1], ~bad[:, :ncol + 1], BOUND[impl])
+    _stable_check(got[:, ncol + 1:], want[:, ncol + 1:], ~bad[:, ncol + 1:], 10 * BOUND[impl], frac=1e-3, hard=1.0)
+    print("\ntextures %s %s colors %d %s" % (impl, name, colors, json.dumps(rec)))
+    assert api.tc_status() == 0
+
+
+@pytest.mark.parametrize("impl", ["tc_fp16", "tc_bf16"])
+@pytest.mark.parametrize("name", ["A256", "hdr512"])
+def test_generate_rbga_tc(frames, oracle, impl, name):
+    """the overlapped RGBA image through generate_RBGA_tc against the oracle
+    on stable pixels, and its window and lists against the plain call"""
+    import conditioning
+    import gpu_runner as R
+    from tile_processor_gpu_b200 import api
+    from test_gpu_parity import _rgba_stable
+    fr, clt = frames[name]
+    c = fr.case
+    fr.set_clt(clt)
+    b, woi, stride, rows = R.rgba(fr, impl=impl)
+    p, woi_p, _, _ = R.rgba(fr)
+    assert np.array_equal(woi, woi_p)
+    o, _, _, _, woi_o = oracle.generate_RBGA(c.geom, c.tasks, c.TX, c.TY, clt, c.port_offsets, stride, rows + 8)
+    assert np.array_equal(woi, woi_o)
+    h, w = (woi[3] + 1) * 8, (woi[2] + 1) * 8
+    keep = _rgba_stable(oracle, fr, [x.astype(np.float64) for x in clt], woi)
+    sl = lambda a: a[:4 * h, :w].reshape(4, h, w)[None]
+    rec = _stable_check(sl(b), sl(o), sl(keep), BOUND[impl], frac=4e-4)
+    print("\ngenerate_RBGA %s %s %s" % (impl, name, json.dumps(rec)))
+    assert api.tc_status() == 0
+
+
+@pytest.mark.parametrize("impl", ["tc_fp16", "tc_bf16"])
+@pytest.mark.parametrize("peak", [1.0, 1e4])
+def test_precision_pipeline_against_fp64(native, oracle, impl, peak):
+    """The whole precision form, each stage fed by the one before it (CLT ->
+    correlation -> textures), against the FP64 oracle run from the same
+    inputs: per-stage largest and RMS error relative to the oracle's largest
+    magnitude (textures: colour slices on stable pixels), on an ordinary and
+    an HDR scene (values up to 1e4)."""
+    import conditioning
+    import gpu_runner as R
+    from tile_processor_gpu_b200 import api
+    c = Case(512, 384, seed=31, border_mode=0, scene="plane", peak=peak)
+    fr = R.Frame(c)
+    clt = R.convert(fr, impl=impl)
+    clt_o = oracle.convert_correct_tiles(c.geom, c.extra, c.kernels, c.pitched, c.dstride, c.tasks)
+    e = {"clt_max": max(rel_err(clt[k], clt_o[k]) for k in range(4)),
+         "clt_rms": max(rms_err(clt[k], clt_o[k]) for k in range(4))}
+    corr = R.correlate(fr, c.corr_idx, stride=225, impl=impl)
+    corr_o = oracle.correlate2D(c.geom, clt_o, 3, .25, .25, .5, 0.05, c.corr_idx, 225, 7)
+    e["corr_max"], e["corr_rms"] = rel_err(corr, corr_o), rms_err(corr, corr_o)
+    tex = R.textures_tiles(fr, c.tex_idx, impl=impl)
+    bad, tex_o = conditioning.unstable_mask(oracle, c, clt_o, c.tex_idx, 0)
+    keep = ~bad[:, :3]
+    den = np.abs(tex_o[:, :3]).max()
+    err = np.abs(tex[:, :3] - tex_o[:, :3])[keep] / den
+    e["texture_max"], e["texture_rms"] = float(err.max()), float(np.sqrt(np.mean(err ** 2)))
+    e["texture_stable_fraction"] = float(keep.mean())
+    print("\nprecision form %s peak %g %s" % (impl, peak, json.dumps({k: float("%.3g" % v) for k, v in e.items()})))
+    assert api.tc_status() == 0
+    assert e["clt_max"] < BOUND[impl] and e["corr_max"] < BOUND[impl]
+    assert e["texture_stable_fraction"] > 0.99
+    assert float((err > BOUND[impl]).mean()) <= 1e-4 and err.max() < 1e-3

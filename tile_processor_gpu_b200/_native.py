@@ -85,6 +85,14 @@ SIGNATURES = {
     "tp_tiles_ya": [_G],
     "tp_set_launch_shape": [_I, _I],
     "tp_get_launch_shape": [_I],
+    "tp_correlate2D_tc": [_G, _P, _I, _F, _F, _F, _F, _S, _P, _S, _I, _P, _I, _P],
+    "tp_convert_correct_tiles_tc": [_G, _P, _P, _P, _P, _P, _S, _I, _I, _I, _P],
+    "tp_textures_accumulate_tc": [_G, _P, _P, _S, _P, _P, _I, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, _I,
+                                  _S, _P, _S, _P, _P, _I, _P],
+    "tp_generate_RBGA_tc": [_G, _P, _I, _P, _P, _P, _I, _I, _P, _P, _I, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I,
+                            _I, _S, _P, _P, _I, _P],
+    "tp_tc_status": [_P, _I],
+    "tp_tc_table_image": [_I, _I, _P],
 }
 STRING_FUNCS = ("tp_last_error", "tp_version")
 # entry points returning a count (long long) instead of a status

@@ -114,6 +114,68 @@ def correlate2D(geom, gpu_clt, colors, scale0, scale1, scale2, fat_zero, num_cor
                  int(corr_radius), _dptr(gpu_corrs), _stream(stream))
 
 
+TC_FP16X2, TC_BF16X2 = 0, 1
+
+
+def correlate2D_tc(geom, gpu_clt, colors, scale0, scale1, scale2, fat_zero, num_corr_tiles, gpu_corr_indices,
+                   corr_stride, corr_radius, gpu_corrs, fmt=TC_FP16X2, stream=None):
+    """correlate2D with the pixel-domain transforms on the tensor cores
+    (split 16-bit operands: fmt TC_FP16X2 or TC_BF16X2)."""
+    _native.call("tp_correlate2D_tc", geom.ptr, _parr(gpu_clt), int(colors), float(scale0), float(scale1),
+                 float(scale2), float(fat_zero), int(num_corr_tiles), _dptr(gpu_corr_indices), int(corr_stride),
+                 int(corr_radius), _dptr(gpu_corrs), int(fmt), _stream(stream))
+
+
+def convert_correct_tiles_tc(geom, gpu_kernel_offsets, gpu_kernels, gpu_images, gpu_tasks, gpu_clt, dstride,
+                             num_tiles, lpf_mask=0, fmt=TC_FP16X2, stream=None):
+    """convert_correct_tiles with the 2-D DCT-IV / DST-IV on the tensor cores."""
+    _native.call("tp_convert_correct_tiles_tc", geom.ptr, _parr(gpu_kernel_offsets), _parr(gpu_kernels),
+                 _parr(gpu_images), _dptr(gpu_tasks), _parr(gpu_clt), int(dstride), int(num_tiles),
+                 int(lpf_mask), int(fmt), _stream(stream))
+
+
+def textures_accumulate_tc(geom, woi, gpu_clt, num_texture_tiles, gpu_texture_indices, gpu_port_offsets, colors,
+                           is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold, min_agree, weight0, weight1,
+                           weight2, dust_remove, keep_weights, texture_rbg_stride, gpu_texture_rbg, texture_stride,
+                           gpu_texture_tiles, gpu_tile_scratch, fmt=TC_FP16X2, stream=None):
+    """textures_accumulate with the inverse CLT on the tensor cores (into gpu_tile_scratch)."""
+    _native.call("tp_textures_accumulate_tc", geom.ptr, _dptr(woi), _parr(gpu_clt), int(num_texture_tiles),
+                 _dptr(gpu_texture_indices), _dptr(gpu_port_offsets), int(colors), int(is_lwir), float(min_shot),
+                 float(scale_shot), float(diff_sigma), float(diff_threshold), float(min_agree), float(weight0),
+                 float(weight1), float(weight2), int(dust_remove), int(keep_weights), int(texture_rbg_stride),
+                 _dptr(gpu_texture_rbg), int(texture_stride), _dptr(gpu_texture_tiles), _parr(gpu_tile_scratch),
+                 int(fmt), _stream(stream))
+
+
+def generate_RBGA_tc(geom, gpu_tasks, num_tiles, gpu_texture_indices, num_texture_tiles, woi, width, height,
+                     gpu_clt, gpu_port_offsets, colors, is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold,
+                     min_agree, weight0, weight1, weight2, dust_remove, keep_weights, texture_rbga_stride,
+                     gpu_texture_tiles, gpu_tile_scratch, fmt=TC_FP16X2, stream=None):
+    """generate_RBGA with the inverse CLT on the tensor cores (into gpu_tile_scratch)."""
+    _native.call("tp_generate_RBGA_tc", geom.ptr, _dptr(gpu_tasks), int(num_tiles), _dptr(gpu_texture_indices),
+                 _dptr(num_texture_tiles), _dptr(woi), int(width), int(height), _parr(gpu_clt),
+                 _dptr(gpu_port_offsets), int(colors), int(is_lwir), float(min_shot), float(scale_shot),
+                 float(diff_sigma), float(diff_threshold), float(min_agree), float(weight0), float(weight1),
+                 float(weight2), int(dust_remove), int(keep_weights), int(texture_rbga_stride),
+                 _dptr(gpu_texture_tiles), _parr(gpu_tile_scratch), int(fmt), _stream(stream))
+
+
+def tc_status(clear=True):
+    """1 when a tensor-core stage kernel's bounded wait ran out since the last clear"""
+    v = ctypes.c_int(0)
+    _native.call("tp_tc_status", ctypes.byref(v), int(bool(clear)))
+    return v.value
+
+
+def tc_table_image(fmt, stage):
+    """The 64 KB shared-memory image of the split transform matrices of a
+    stage (0 correlation, 1 inverse CLT, 2 forward CLT) as uint16 [32768]
+    (host-side, no device needed)."""
+    out = np.zeros(32768, dtype=np.uint16)
+    _native.call("tp_tc_table_image", int(fmt), int(stage), out.ctypes.data_as(ctypes.c_void_p))
+    return out
+
+
 def textures_accumulate(geom, woi, gpu_clt, num_texture_tiles, gpu_texture_indices, gpu_port_offsets, colors,
                         is_lwir, min_shot, scale_shot, diff_sigma, diff_threshold, min_agree, weight0, weight1,
                         weight2, dust_remove, keep_weights, texture_rbg_stride, gpu_texture_rbg, texture_stride,

@@ -27,6 +27,9 @@
 #include "tp_frame.cuh"
 #include "tp_disparity.cuh"
 #include "tp_kernels_gen.cuh"
+#include "tp_corr_tc.cuh"
+#include "tp_inv_tc.cuh"
+#include "tp_fwd_tc.cuh"
 #include "tp_mlp.cuh"
 
 #define TP_VERSION "tile_processor_gpu_b200 0.1 (sm_100a)"
@@ -114,7 +117,7 @@ int shape_per_sm(int which)
  * their attribute once per device (the first call; make it before capturing
  * a stream into a graph). */
 std::mutex g_attr_mutex;
-bool g_tex_attr[128], g_frame_attr[128], g_tc_attr[128];
+bool g_tex_attr[128], g_tex_t_attr[128], g_frame_attr[128], g_tc_attr[128];
 
 int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
 {
@@ -132,8 +135,11 @@ int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
 
 int texture_smem_setup()
 {
-    return set_smem_once(g_tex_attr, (const void *)tp::k_textures, tp::kTexSmemBytes,
-                         "cudaFuncSetAttribute(k_textures)");
+    const int rc = set_smem_once(g_tex_attr, (const void *)tp::k_textures<false>, tp::kTexSmemBytes,
+                                 "cudaFuncSetAttribute(k_textures)");
+    if (rc) return rc;
+    return set_smem_once(g_tex_t_attr, (const void *)tp::k_textures<true>, tp::kTexSmemBytes,
+                         "cudaFuncSetAttribute(k_textures<tiles>)");
 }
 
 /* Scratch of tp_generate_RBGA_noalloc: [0, 8) sub-list counts, [8, 12) window
@@ -364,7 +370,7 @@ int tp_textures_accumulate(const tp_geometry *g, const int *woi, float *const *c
     if ((rc = sm_count(&sms))) return rc;
     if ((rc = texture_smem_setup())) return rc;
     unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
-    tp::k_textures<<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
+    tp::k_textures<false><<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
         gd, woi, clt, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
         want_tiles ? texture_tiles : nullptr);
@@ -495,11 +501,17 @@ int tp_clear_texture_rbga(const tp_geometry *g, int texture_width, int texture_s
     return cuda_status(cudaGetLastError(), "clear_texture_rbga launch");
 }
 
+static int inv_tc_launch(const tp::InvTcStage &st, int format, tp_stream_t stream);
+
+/* tile_scratch / format: when format >= 0, the inverse CLT of every listed
+ * tile runs first on the tensor cores (InvTcStage) into tile_scratch, and
+ * the passes read those tiles (k_textures<true>) */
 static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
                          int *num_texture_tiles, int *woi, int width, int height, float *const *clt,
                          const float *port_offsets, int colors, float min_shot, float scale_shot, float diff_sigma,
                          float weight0, float weight1, float weight2, int dust_remove, size_t texture_rbga_stride,
-                         float *texture_tiles, int row_first, int row_last, tp_stream_t stream)
+                         float *texture_tiles, int row_first, int row_last, float *const *tile_scratch, int format,
+                         tp_stream_t stream)
 {
     tp::Geom gd;
     int rc = check_geometry(g, &gd);
@@ -533,6 +545,13 @@ static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, in
                                                (const int *)woi, colors, 0, 0, texture_rbga_stride, texture_tiles);
         if (err != cudaSuccess) return cuda_status(err, "generate_RBGA clear launch");
     }
+    float *const *src = clt;
+    if (format >= 0) {
+        /* an ordinary launch: it reads the tasks the list kernels rewrote */
+        tp::InvTcStage st{gd, clt, tile_scratch, tasks, (long long)num_tiles, nullptr, colors};
+        if ((rc = inv_tc_launch(st, format, stream))) return rc;
+        src = tile_scratch;
+    }
     const int quarter = gd.TX * (gd.TYA >> 2);
     const unsigned grid = grid_for(quarter, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
     /* one pass per tile parity: its inner sub-list, then its border one (the
@@ -540,10 +559,16 @@ static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, in
      * tiles of one parity never overlap, so a pass needs no ordering) */
     for (int parity = 0; parity < 4; parity++) {
         const int *base = texture_indices + parity * quarter;
-        const cudaError_t err = launch_chained(
-            true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures, gd, (const int *)woi, clt, 0LL,
-            (const int *)base, (const int *)num_texture_tiles, parity << 1, quarter, -quarter, port_offsets, p,
-            texture_rbga_stride, texture_tiles, (size_t)0, (float *)nullptr);
+        const cudaError_t err =
+            format >= 0
+                ? launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures<true>, gd,
+                                 (const int *)woi, src, 0LL, (const int *)base, (const int *)num_texture_tiles,
+                                 parity << 1, quarter, -quarter, port_offsets, p, texture_rbga_stride, texture_tiles,
+                                 (size_t)0, (float *)nullptr)
+                : launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures<false>, gd,
+                                 (const int *)woi, src, 0LL, (const int *)base, (const int *)num_texture_tiles,
+                                 parity << 1, quarter, -quarter, port_offsets, p, texture_rbga_stride, texture_tiles,
+                                 (size_t)0, (float *)nullptr);
         if (err != cudaSuccess) return cuda_status(err, "generate_RBGA texture pass launch");
     }
     return cuda_status(cudaGetLastError(), "generate_RBGA launch");
@@ -559,7 +584,7 @@ int tp_generate_RBGA(const tp_geometry *g, tp_task *tasks, int num_tiles, int *t
     (void)is_lwir; (void)diff_threshold; (void)min_agree; (void)keep_weights;
     return generate_rbga(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height, clt,
                          port_offsets, colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2,
-                         dust_remove, texture_rbga_stride, texture_tiles, 0, INT_MAX, stream);
+                         dust_remove, texture_rbga_stride, texture_tiles, 0, INT_MAX, nullptr, -1, stream);
 }
 
 int tp_generate_RBGA_rows(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
@@ -573,7 +598,8 @@ int tp_generate_RBGA_rows(const tp_geometry *g, tp_task *tasks, int num_tiles, i
         return fail(TP_ERR_ARG, "tile rows [%d, %d)", row_first, row_last);
     return generate_rbga(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height, clt,
                          port_offsets, colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2,
-                         dust_remove, texture_rbga_stride, texture_tiles, row_first, row_last, stream);
+                         dust_remove, texture_rbga_stride, texture_tiles, row_first, row_last, nullptr, -1,
+                         stream);
 }
 
 int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *const *kernels, float *const *images,
@@ -845,6 +871,292 @@ int tp_disparity_fit(const tp_geometry *g, const float *corrs, size_t corr_strid
                                                                (long long)num_corr_tiles, corr_indices,
                                                                port_offsets, pair_mask, mode, disparity, strength);
     return cuda_status(cudaGetLastError(), "disparity_fit launch");
+}
+
+} /* extern "C" */
+
+/* ---- tensor-core (hi + lo split) forms of the CLT stages -------------------
+ *
+ * The 64 x 64 matrices K_q = V_q (x) H_q of each stage's four quadrant
+ * transforms, split into two 16-bit halves (hi = K rounded to the format,
+ * lo = (K - hi) rounded) and stored as the 128-byte-swizzled B images the
+ * kernels copy into shared memory (tp_tc_engine.cuh): per format and stage
+ * 64 KB, the four hi quadrants then the four lo.  Built on the host in
+ * double from the closed forms of the 8-point transforms, copied once per
+ * device (and again after a device reset) on the first tensor-core call;
+ * make that first call before any stream capture. */
+enum { kTcStageCorr = 0, kTcStageInv = 1, kTcStageFwd = 2, kTcStagesN = 3 };
+static __device__ __align__(1024) unsigned char g_tc_btab[2][kTcStagesN][tp::kTcBBytes];
+/* set by a tensor-core kernel whose bounded wait ran out (tp_tc_status) */
+static __device__ int g_tc_err;
+
+namespace {
+
+/* M[k][n] of the four 8-point transforms (DCT-IV, DST-IV, DCT-II, DST-II) */
+double tc_dtt(int kind, int k, int n)
+{
+    const double pi = 3.14159265358979323846;
+    switch (kind) {
+    case 0: return 0.5 * cos(pi * (2 * k + 1) * (2 * n + 1) / 32.0);
+    case 1: return 0.5 * sin(pi * (2 * k + 1) * (2 * n + 1) / 32.0);
+    case 2: return 0.5 * cos(pi * (2 * n + 1) * k / 16.0);
+    default: return 0.5 * sin(pi * (2 * n + 1) * (k + 1) / 16.0);
+    }
+}
+
+/* vertical / horizontal transform kinds of quadrant q of a stage (-1: unused) */
+void tc_kinds(int stage, int q, int *v, int *h)
+{
+    if (stage == kTcStageCorr) { /* correlate2D: DCT-II / DST-II, q1 and q3 sine horizontally, q2 and q3 vertically */
+        *v = 2 + (q >> 1);
+        *h = 2 + (q & 1);
+    } else if (stage == kTcStageInv) { /* inverse CLT: DCT-IV / DST-IV in the same pattern */
+        *v = q >> 1;
+        *h = q & 1;
+    } else { /* forward CLT: slot 0 CC (DCT-IV both ways), slot 1 SC (DST-IV horizontally) */
+        *v = q < 2 ? 0 : -1;
+        *h = q < 2 ? q : -1;
+    }
+}
+
+uint16_t tc_half_bits(double x, int fmt)
+{
+    if (fmt == TP_TC_BF16X2) return __bfloat16_as_ushort(__double2bfloat16(x));
+    return __half_as_ushort(__double2half(x));
+}
+
+double tc_half_value(uint16_t b, int fmt)
+{
+    if (fmt == TP_TC_BF16X2) return (double)__bfloat162float(__ushort_as_bfloat16(b));
+    return (double)__half2float(__ushort_as_half(b));
+}
+
+void tc_build_table(int fmt, int stage, uint16_t *img)
+{
+    memset(img, 0, tp::kTcBBytes);
+    for (int q = 0; q < 4; q++) {
+        int kv, kh;
+        tc_kinds(stage, q, &kv, &kh);
+        if (kv < 0) continue;
+        for (int i = 0; i < 8; i++)
+            for (int j = 0; j < 8; j++)
+                for (int m = 0; m < 8; m++)
+                    for (int n = 0; n < 8; n++) {
+                        const double x = tc_dtt(kv, i, m) * tc_dtt(kh, j, n);
+                        const uint16_t hi = tc_half_bits(x, fmt);
+                        const uint16_t lo = tc_half_bits(x - tc_half_value(hi, fmt), fmt);
+                        const uint32_t off = tp::tc_sw_off(i * 8 + j, m * 8 + n);
+                        img[(q * tp::kTcBQuadBytes + off) / 2] = hi;
+                        img[((4 + q) * tp::kTcBQuadBytes + off) / 2] = lo;
+                    }
+    }
+}
+
+std::mutex g_tcb_mutex;
+unsigned long long g_tcb_ctx[128];
+bool g_tcb_ready[128];
+
+/* the B tables on the current device (built and copied on first use) and the
+ * device address of the table of (fmt, stage) */
+int tc_tables(int fmt, int stage, const unsigned char **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(TP_ERR_NO_DEVICE, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= 128) return fail(TP_ERR_NO_DEVICE, "device %d", dev);
+    std::lock_guard<std::mutex> lock(g_tcb_mutex);
+    const unsigned long long ctx = current_context_id();
+    if (!g_tcb_ready[dev] || ctx == 0 || ctx != g_tcb_ctx[dev]) {
+        static uint16_t img[2][kTcStagesN][tp::kTcBTableHalves];
+        for (int f = 0; f < 2; f++)
+            for (int st = 0; st < kTcStagesN; st++) tc_build_table(f, st, img[f][st]);
+        e = cudaMemcpyToSymbol(g_tc_btab, img, sizeof(img));
+        if (e != cudaSuccess) return fail(TP_ERR_CUDA, "tensor-core tables: %s", cudaGetErrorString(e));
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(zero));
+        if (e != cudaSuccess) return fail(TP_ERR_CUDA, "tensor-core status: %s", cudaGetErrorString(e));
+        g_tcb_ready[dev] = true;
+        g_tcb_ctx[dev] = current_context_id();
+    }
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_tc_btab);
+    if (e != cudaSuccess) return fail(TP_ERR_CUDA, "cudaGetSymbolAddress(tables): %s", cudaGetErrorString(e));
+    *out = static_cast<const unsigned char *>(p) + ((size_t)fmt * kTcStagesN + stage) * tp::kTcBBytes;
+    return TP_OK;
+}
+
+int tc_err_ptr(int **out)
+{
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_tc_err);
+    if (e != cudaSuccess) return fail(TP_ERR_CUDA, "cudaGetSymbolAddress(status): %s", cudaGetErrorString(e));
+    *out = static_cast<int *>(p);
+    return TP_OK;
+}
+
+/* the power of two that keeps |x| * scale below 2^15 for |x| <= bound */
+float tc_fp16_scale(double bound)
+{
+    if (!(bound > 0.0)) return 1.0f;
+    int e = 0;
+    (void)frexp(bound, &e); /* bound < 2^e */
+    return ldexpf(1.0f, 15 - e);
+}
+
+bool g_corr_tc_attr[2][128], g_inv_tc_attr[2][128], g_fwd_tc_attr[2][128];
+
+/* one persistent CTA per SM (at most one per 128-row block) of the shared
+ * tensor-core pipeline for stage S */
+template <class S>
+int tc_launch(const S &st, int format, int stage, bool (*attr)[128], tp_stream_t stream, const char *what)
+{
+    const unsigned char *btab = nullptr;
+    int *err = nullptr;
+    int rc;
+    if ((rc = tc_tables(format, stage, &btab)) || (rc = tc_err_ptr(&err))) return rc;
+    constexpr int smem = tp::tc_stage_smem(S::kQuads, S::kMeta);
+    const void *kern = format == TP_TC_BF16X2 ? (const void *)tp::k_tc_stage<S, TP_TC_BF16X2>
+                                              : (const void *)tp::k_tc_stage<S, TP_TC_FP16X2>;
+    if ((rc = set_smem_once(attr[format], kern, smem, what))) return rc;
+    const long long blocks = (st.rows() + tp::kTcRows - 1) / tp::kTcRows;
+    if (blocks <= 0) return TP_OK;
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    const unsigned grid = (unsigned)(blocks < sms ? blocks : sms);
+    if (format == TP_TC_BF16X2)
+        tp::k_tc_stage<S, TP_TC_BF16X2><<<grid, S::kThreads, smem, (cudaStream_t)stream>>>(st, btab, err);
+    else
+        tp::k_tc_stage<S, TP_TC_FP16X2><<<grid, S::kThreads, smem, (cudaStream_t)stream>>>(st, btab, err);
+    return cuda_status(cudaGetLastError(), what);
+}
+
+} /* namespace */
+
+static int inv_tc_launch(const tp::InvTcStage &st, int format, tp_stream_t stream)
+{
+    return tc_launch(st, format, kTcStageInv, g_inv_tc_attr, stream, "inverse CLT (tensor cores)");
+}
+
+extern "C" {
+
+int tp_tc_status(int *timed_out, int clear)
+{
+    if (!timed_out) return fail(TP_ERR_ARG, "timed_out is NULL");
+    const unsigned char *unused;
+    int rc = tc_tables(0, 0, &unused);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyFromSymbol(timed_out, g_tc_err, sizeof(int));
+    if (e != cudaSuccess) return fail(TP_ERR_CUDA, "tensor-core status: %s", cudaGetErrorString(e));
+    if (clear) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(zero));
+        if (e != cudaSuccess) return fail(TP_ERR_CUDA, "tensor-core status: %s", cudaGetErrorString(e));
+    }
+    return TP_OK;
+}
+
+int tp_tc_table_image(int format, int stage, void *out)
+{
+    if (format != TP_TC_FP16X2 && format != TP_TC_BF16X2) return fail(TP_ERR_ARG, "format %d", format);
+    if (stage < 0 || stage >= kTcStagesN) return fail(TP_ERR_ARG, "stage %d", stage);
+    if (!out) return fail(TP_ERR_ARG, "out is NULL");
+    tc_build_table(format, stage, static_cast<uint16_t *>(out));
+    return TP_OK;
+}
+
+int tp_convert_correct_tiles_tc(const tp_geometry *g, float *const *kernel_offsets, float *const *kernels,
+                                float *const *images, const tp_task *tasks, float *const *clt, size_t dstride,
+                                int num_tiles, int lpf_mask, int format, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (format != TP_TC_FP16X2 && format != TP_TC_BF16X2) return fail(TP_ERR_ARG, "format %d", format);
+    if (!kernel_offsets || !kernels || !images || !clt) return fail(TP_ERR_ARG, "NULL pointer array");
+    if (num_tiles < 0) return fail(TP_ERR_ARG, "num_tiles %d < 0", num_tiles);
+    if (num_tiles > 0 && !tasks) return fail(TP_ERR_ARG, "tasks is NULL");
+    if (dstride < (size_t)g->img_width) return fail(TP_ERR_ARG, "dstride %zu < width %d", dstride, g->img_width);
+    if (num_tiles == 0) return TP_OK;
+    const tp::FwdTcStage st{gd, dstride, kernel_offsets, kernels, images, tasks, clt, num_tiles, lpf_mask};
+    return tc_launch(st, format, kTcStageFwd, g_fwd_tc_attr, stream, "convert_correct_tiles_tc");
+}
+
+int tp_correlate2D_tc(const tp_geometry *g, float *const *clt, int colors, float scale0, float scale1,
+                      float scale2, float fat_zero, size_t num_corr_tiles, const int *corr_indices,
+                      size_t corr_stride, int corr_radius, float *corrs, int format, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (format != TP_TC_FP16X2 && format != TP_TC_BF16X2) return fail(TP_ERR_ARG, "format %d", format);
+    if (!clt) return fail(TP_ERR_ARG, "clt is NULL");
+    if (colors != 1 && colors != 3) return fail(TP_ERR_ARG, "colors %d (1 or 3)", colors);
+    if (corr_radius < 0 || corr_radius > TP_MAX_CORR_RADIUS)
+        return fail(TP_ERR_ARG, "corr_radius %d outside 0..%d", corr_radius, TP_MAX_CORR_RADIUS);
+    const size_t sz = (size_t)(2 * corr_radius + 1) * (2 * corr_radius + 1);
+    if (num_corr_tiles == 0) return TP_OK;
+    if (!corr_indices || !corrs) return fail(TP_ERR_ARG, "NULL corr_indices / corrs");
+    if (corr_stride < sz) return fail(TP_ERR_ARG, "corr_stride %zu < (2r+1)^2 = %zu", corr_stride, sz);
+    /* the final LPF bounds the normalised product */
+    double bound = 0.0;
+    for (int i = 0; i < 64; i++) bound = fmax(bound, fabs((double)g_lpf_host[5][i]));
+    const float up = format == TP_TC_FP16X2 ? tc_fp16_scale(bound) : 1.0f;
+    const tp::CorrTcStage st{gd, clt, colors, scale0, scale1, scale2, fat_zero, (long long)num_corr_tiles,
+                             corr_indices, corr_stride, corr_radius, corrs, up};
+    return tc_launch(st, format, kTcStageCorr, g_corr_tc_attr, stream, "correlate2D_tc");
+}
+
+int tp_textures_accumulate_tc(const tp_geometry *g, const int *woi, float *const *clt, size_t num_texture_tiles,
+                              const int *texture_indices, const float *port_offsets, int colors, int is_lwir,
+                              float min_shot, float scale_shot, float diff_sigma, float diff_threshold,
+                              float min_agree, float weight0, float weight1, float weight2, int dust_remove,
+                              int keep_weights, size_t texture_rbg_stride, float *texture_rbg, size_t texture_stride,
+                              float *texture_tiles, float *const *tile_scratch, int format, tp_stream_t stream)
+{
+    (void)is_lwir; (void)diff_threshold; (void)min_agree; /* accepted, unused (as in the reference) */
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (format != TP_TC_FP16X2 && format != TP_TC_BF16X2) return fail(TP_ERR_ARG, "format %d", format);
+    tp::TextureParams p;
+    if ((rc = texture_params(colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2, dust_remove,
+                             keep_weights, &p)))
+        return rc;
+    if (num_texture_tiles == 0) return TP_OK;
+    if (!clt || !texture_indices || !port_offsets || !tile_scratch)
+        return fail(TP_ERR_ARG, "NULL clt / indices / port_offsets / tile_scratch");
+    const bool want_rbg = texture_rbg && texture_rbg_stride;
+    const bool want_tiles = texture_tiles && texture_stride;
+    if (want_rbg && !woi) return fail(TP_ERR_ARG, "woi is NULL with an RGBA image output");
+    const int ns = (colors == 3) ? (keep_weights ? 12 : 4) : (keep_weights ? 8 : 2);
+    if (want_tiles && texture_stride < (size_t)ns * 256)
+        return fail(TP_ERR_ARG, "texture_stride %zu < %d slices x 256", texture_stride, ns);
+    const tp::InvTcStage st{gd, clt, tile_scratch, nullptr, (long long)num_texture_tiles, texture_indices, colors};
+    if ((rc = inv_tc_launch(st, format, stream))) return rc;
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    if ((rc = texture_smem_setup())) return rc;
+    unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
+    tp::k_textures<true><<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
+        gd, woi, tile_scratch, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
+        want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
+        want_tiles ? texture_tiles : nullptr);
+    return cuda_status(cudaGetLastError(), "textures_accumulate_tc launch");
+}
+
+int tp_generate_RBGA_tc(const tp_geometry *g, tp_task *tasks, int num_tiles, int *texture_indices,
+                        int *num_texture_tiles, int *woi, int width, int height, float *const *clt,
+                        const float *port_offsets, int colors, int is_lwir, float min_shot, float scale_shot,
+                        float diff_sigma, float diff_threshold, float min_agree, float weight0, float weight1,
+                        float weight2, int dust_remove, int keep_weights, size_t texture_rbga_stride,
+                        float *texture_tiles, float *const *tile_scratch, int format, tp_stream_t stream)
+{
+    (void)is_lwir; (void)diff_threshold; (void)min_agree; (void)keep_weights;
+    if (format != TP_TC_FP16X2 && format != TP_TC_BF16X2) return fail(TP_ERR_ARG, "format %d", format);
+    if (!tile_scratch) return fail(TP_ERR_ARG, "tile_scratch is NULL");
+    return generate_rbga(g, tasks, num_tiles, texture_indices, num_texture_tiles, woi, width, height, clt,
+                         port_offsets, colors, min_shot, scale_shot, diff_sigma, weight0, weight1, weight2,
+                         dust_remove, texture_rbga_stride, texture_tiles, 0, INT_MAX, tile_scratch, format, stream);
 }
 
 } /* extern "C" */

@@ -46,21 +46,20 @@ struct ConvertJob {
     int cam, color;
 };
 
-/* STREAM: out is global memory and takes evict-first stores.  The kernel
- * writes 963 MB of CLT for a full quad frame, far more than L2 holds, and
- * later kernels read it back; retaining the stores in L2 would only evict the
- * kernel tiles and Bayer rows that neighbouring jobs of this kernel still
- * read. */
-template <bool STREAM = false>
-__device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
-                                            const float *__restrict__ extra_tab,
-                                            const float *__restrict__ kern_tab,
-                                            const float *__restrict__ img, float cx, float cy,
-                                            int color, int lpf_mask, float *__restrict__ out,
-                                            float (*tb)[9], int l, unsigned gm, const float *pre_ex = nullptr)
+/* Where a job's window sits and how its kernel tile and shifts follow from
+ * the task's tile centre (float32, as the reference computes them:
+ * src/TileProcessor.cuh:3129-3255). */
+struct JobGeometry {
+    size_t kidx;    /* kernel tile (x, y, colour) index into the table   */
+    int itlx, itly; /* integer corner of the 16x16 window                */
+    float shx, shy; /* residual shifts                                   */
+    float hc, hs, vc, vs; /* (cos, sin)(pi s / 16) of the shifted windows */
+};
+
+__device__ __forceinline__ JobGeometry job_geometry(const Geom &g, const float *__restrict__ extra_tab, float cx,
+                                                    float cy, int color, const float *pre_ex)
 {
-    /* ---- kernel tile, integer corner, residual shift (float32, as the
-     * reference computes them: src/TileProcessor.cuh:3129-3255) ---- */
+    JobGeometry j;
     const float step_inv = __int_as_float((127 - g.ls) << 23);
     int ktx = __float2int_rn(__fmaf_rn(cx, step_inv, 1.0f));
     int kty = __float2int_rn(__fmaf_rn(cy, step_inv, 1.0f));
@@ -68,31 +67,36 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
     kty = min(g.KV - 1, max(0, kty));
     const float kdx = (cx - (float)(ktx << g.ls)) + (float)(1 << (g.ls - 1));
     const float kdy = (cy - (float)(kty << g.ls)) + (float)(1 << (g.ls - 1));
-    const size_t kidx = ((size_t)ktx + (size_t)kty * g.KH) * 3 + color;
+    j.kidx = ((size_t)ktx + (size_t)kty * g.KH) * 3 + color;
     /* the kernel tile's offsets: prefetched by the caller (pre_ex[6]) or here */
-    const float *ex = extra_tab + kidx * 8;
+    const float *ex = extra_tab + j.kidx * 8;
     const float data_x = pre_ex ? pre_ex[0] : __ldg(ex + 0), data_y = pre_ex ? pre_ex[1] : __ldg(ex + 1);
     const float dxc_dx = pre_ex ? pre_ex[2] : __ldg(ex + 4), dxc_dy = pre_ex ? pre_ex[3] : __ldg(ex + 5);
     const float dyc_dx = pre_ex ? pre_ex[4] : __ldg(ex + 6), dyc_dy = pre_ex ? pre_ex[5] : __ldg(ex + 7);
     const float px = (cx - 8.0f) - __fmaf_rn(dxc_dy, kdy, __fmaf_rn(dxc_dx, kdx, data_x));
     const float py = (cy - 8.0f) - __fmaf_rn(dyc_dy, kdy, __fmaf_rn(dyc_dx, kdx, data_y));
-    const int itlx = corner_clamp(__float2int_rd(px + 0.5f), g.W, true, g.border_mode);
-    const int itly = corner_clamp(__float2int_rd(py + 0.5f), g.H, false, g.border_mode);
-    const float shx = (float)itlx - px;
-    const float shy = (float)itly - py;
-
+    j.itlx = corner_clamp(__float2int_rd(px + 0.5f), g.W, true, g.border_mode);
+    j.itly = corner_clamp(__float2int_rd(py + 0.5f), g.H, false, g.border_mode);
+    j.shx = (float)j.itlx - px;
+    j.shy = (float)j.itly - py;
     /* (cos, sin)(pi s / 16) for the shifted windows */
-    const float xh = shx * (1.0f / 16.0f), xv = shy * (1.0f / 16.0f);
-    float hc, hs, vc, vs;
-    sincospif(xh, &hs, &hc);
-    sincospif(xv, &vs, &vc);
+    const float xh = j.shx * (1.0f / 16.0f), xv = j.shy * (1.0f / 16.0f);
+    sincospif(xh, &j.hs, &j.hc);
+    sincospif(xv, &j.vs, &j.vc);
+    return j;
+}
 
+/* The fold: lane l builds DTT row l of the folded, windowed Bayer samples of
+ * the job's colour (P: the cosine fold; Q: the sine-windowed fold of green,
+ * zeros for red and blue), both Bayer phases of green summed
+ * (src/TileProcessor.cuh:3257-3416). */
+__device__ __forceinline__ void fold_rows(const Geom &g, size_t dstride, const float *__restrict__ img,
+                                          const JobGeometry &j, int color, int l, float P[8], float Q[8])
+{
+    const int itlx = j.itlx, itly = j.itly;
     const int c0 = color & 1, c1 = (color >> 1) & 1;
     const bool fast = (itlx >= 0) && (itlx < g.W - 16) && (itly >= 0) && (itly < g.H - 16);
     const long long last = (long long)g.image_rows * (long long)dstride - 1;
-
-    /* ---- fold: lane l builds DTT row l ---- */
-    float P[8], Q[8];
 #pragma unroll
     for (int v = 0; v < 8; v++) { P[v] = 0.0f; Q[v] = 0.0f; }
 #pragma unroll
@@ -101,7 +105,7 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
         const int colp = (itlx & 1) ^ (1 ^ c0 ^ c1 ^ gp);
         const int rowp = (itly & 1) ^ (c0 ^ gp);
         const int lr = fold_sample(l, rowp);
-        const float wv = fold_sign_c(lr) * shifted_window_lane(lr, vc, vs);
+        const float wv = fold_sign_c(lr) * shifted_window_lane(lr, j.vc, j.vs);
         long long rowbase;
         int eff_col = 0;
         if (fast) {
@@ -120,7 +124,7 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
 #pragma unroll
         for (int v = 0; v < 8; v++) {
             const int lc = fold_sample(v, colp);
-            const float whs_raw = shifted_window(lc, hc, hs);
+            const float whs_raw = shifted_window(lc, j.hc, j.hs);
             float pix;
             if (fast) {
                 pix = __ldg(img + rowbase + lc);
@@ -136,6 +140,30 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
             if (c1) Q[v] = __fmaf_rn(d, fold_sign_s(lc) * whs_raw, Q[v]);
         }
     }
+}
+
+/* STREAM: out is global memory and takes evict-first stores.  The kernel
+ * writes 963 MB of CLT for a full quad frame, far more than L2 holds, and
+ * later kernels read it back; retaining the stores in L2 would only evict the
+ * kernel tiles and Bayer rows that neighbouring jobs of this kernel still
+ * read. */
+template <bool STREAM = false>
+__device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
+                                            const float *__restrict__ extra_tab,
+                                            const float *__restrict__ kern_tab,
+                                            const float *__restrict__ img, float cx, float cy,
+                                            int color, int lpf_mask, float *__restrict__ out,
+                                            float (*tb)[9], int l, unsigned gm, const float *pre_ex = nullptr)
+{
+    const JobGeometry jg = job_geometry(g, extra_tab, cx, cy, color, pre_ex);
+    const size_t kidx = jg.kidx;
+    const int itlx = jg.itlx, itly = jg.itly;
+    const float shx = jg.shx, shy = jg.shy;
+    const int c1 = (color >> 1) & 1;
+
+    /* ---- fold: lane l builds DTT row l ---- */
+    float P[8], Q[8];
+    fold_rows(g, dstride, img, jg, color, l, P, Q);
 
     /* ---- 2-D transform: rows (registers), transpose, columns ---- */
     float cc[8], sc[8], cs[8], ss[8], t[8];

@@ -26,6 +26,7 @@
  */
 #pragma once
 #include "tp_common.cuh"
+#include "tp_correlate.cuh"
 
 namespace tp {
 
@@ -321,6 +322,11 @@ constexpr int kTexThreads = 96;
 constexpr int kTexSmemFloats = 12 * kJob + 12 * kTB4;
 constexpr size_t kTexSmemBytes = sizeof(float) * kTexSmemFloats;
 
+/* FROM_T: `clt` holds the jobs' pixel tiles instead of their CLT, as
+ * k_tc_stage<InvTcStage> writes them (the un-windowed T for colour, the
+ * windowed M for mono, [16][16] row-major at the job's CLT offset): stage 1
+ * copies the tile into shared memory instead of inverting the CLT. */
+template <bool FROM_T>
 __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     Geom g, const int *__restrict__ woi, float *const *clt, long long num_texture_tiles,
     const int *__restrict__ list, const int *__restrict__ dev_counts, int count_slot, int list_cap,
@@ -463,7 +469,22 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
         }
 
         /* ---- stages 1-2: per (camera, color) group ---- */
-        if (grp < njobs) {
+        if (grp < njobs && FROM_T) {
+            const int cam = grp / colors, color = grp - cam * colors;
+            float *tj = s_t + grp * kJob, *xj = s_x + grp * kTB4;
+            const float *src = s_cp[cam] + ((size_t)tile * 3 + color) * 256 + l * 32;
+            const bool al16 = !(reinterpret_cast<uintptr_t>(src) & 15);
+            /* lane l: rows 2 l and 2 l + 1 */
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                float v[16];
+                load_row8(src + 16 * h, al16, v);
+                load_row8(src + 16 * h + 8, al16, v + 8);
+#pragma unroll
+                for (int c = 0; c < 16; c++) tj[JT(2 * l + h, c)] = v[c];
+            }
+            if (colors > 1) debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
+        } else if (grp < njobs) {
             const int cam = grp / colors, color = grp - cam * colors;
             float *tj = s_t + grp * kJob, *xj = s_x + grp * kTB4;
             if (colors > 1) {
