@@ -313,19 +313,20 @@ class BatchedFrames:
 class FramePipeline:
     """Device buffers for one frame and the three hot-path calls."""
 
-    def __init__(self, seed=0, device="cuda"):
+    def __init__(self, seed=0, device="cuda", size=(WIDTH, HEIGHT)):
         import torch
         from tile_processor_gpu_b200 import api, synth
         self.api, self.torch = api, torch
         rng = np.random.default_rng(seed)
-        self.geom_d = synth.geometry(WIDTH, HEIGHT, image_rows=HEIGHT + 16)
+        self.W, self.H = W, H = size
+        self.geom_d = synth.geometry(W, H, image_rows=H + 16)
         g = self.g = api.Geometry.from_dict(self.geom_d)
         self.TX, self.TY, self.TYA = synth.tiles(self.geom_d)
-        imgs, disp = synth.plane_scene(rng, WIDTH, HEIGHT, disparity=(0.0, 64.0), texture="detail")
+        imgs, disp = synth.plane_scene(rng, W, H, disparity=(0.0, 64.0), texture="detail")
         self.scene_disparity = disp
-        self.dstride = WIDTH + 64
-        pitched = np.zeros((4, HEIGHT + 16, self.dstride), np.float32)
-        pitched[:, :HEIGHT, :WIDTH] = imgs
+        self.dstride = W + 64
+        pitched = np.zeros((4, H + 16, self.dstride), np.float32)
+        pitched[:, :H, :W] = imgs
         self.host_images = [torch.from_numpy(pitched[c]).pin_memory() for c in range(4)]
         # centred PSFs without kernel-centre offsets: the cameras carry no
         # shift the scene does not have, so the disparity is measurable
@@ -395,6 +396,27 @@ class FramePipeline:
                                self.TY, self.p_clt, self.port_offsets, t["colors"], t["is_lwir"], t["min_shot"],
                                t["scale_shot"], t["diff_sigma"], t["diff_threshold"], t["min_agree"], t["weight0"],
                                t["weight1"], t["weight2"], t["dust_remove"], 0, self.rgba_stride, rgba)
+
+    # the precision form: the same three calls with their 8x8 transforms on the
+    # tensor cores (split FP16 or BF16 operands); the texture call's inverse
+    # CLT goes through a tile buffer of the CLT's size
+    def precision_stage(self, stage, fmt):
+        api, t = self.api, TEXTURE
+        if stage == "convert":
+            api.convert_correct_tiles_tc(self.g, self.p_extra, self.p_kernels, self.p_images, self.tasks, self.p_clt,
+                                         self.dstride, self.num_tiles, 0, fmt=fmt)
+        elif stage == "correlate":
+            api.correlate2D_tc(self.g, self.p_clt, 3, 0.25, 0.25, 0.5, FAT_ZERO, self.num_corr, self.corr_idx,
+                               self.corr_stride, CORR_RADIUS, self.corrs, fmt=fmt)
+        else:
+            if not hasattr(self, "p_tiles"):
+                self.tiles = [self.torch.empty_like(c) for c in self.clt]
+                self.p_tiles = api.PointerArray(self.tiles)
+            api.generate_RBGA_tc(self.g, self.tasks, self.num_tiles, self.tex_indices, self.num_tex, self.woi,
+                                 self.TX, self.TY, self.p_clt, self.port_offsets, t["colors"], t["is_lwir"],
+                                 t["min_shot"], t["scale_shot"], t["diff_sigma"], t["diff_threshold"],
+                                 t["min_agree"], t["weight0"], t["weight1"], t["weight2"], t["dust_remove"], 0,
+                                 self.rgba_stride, self.rgba, self.p_tiles, fmt=fmt)
 
     def add_slot(self, device):
         """Device images and outputs plus pinned host outputs of one more
@@ -500,7 +522,7 @@ class FramePipeline:
         """compulsory HBM bytes of one frame through the fused path: images,
         touched kernel tiles and offsets, tasks, correlation out, RGBA out"""
         T = self.num_tiles
-        return (4 * WIDTH * HEIGHT * 4 + self.kernel_tiles_touched * (1024 + 32) + T * 40 +
+        return (4 * self.W * self.H * 4 + self.kernel_tiles_touched * (1024 + 32) + T * 40 +
                 self.num_corr * self.corr_size * 4 + (self.TX + 1) * 8 * (self.TY + 1) * 8 * 4 * 4)
 
     def algorithmic_bytes(self):
@@ -508,7 +530,7 @@ class FramePipeline:
         T = self.num_tiles
         clt = 4 * T * 3 * 1024
         return {
-            "convert": 4 * WIDTH * HEIGHT * 4 + self.kernel_tiles_touched * (1024 + 32) + T * 40 + clt,
+            "convert": 4 * self.W * self.H * 4 + self.kernel_tiles_touched * (1024 + 32) + T * 40 + clt,
             "correlate": clt + self.num_corr * 4 + self.num_corr * self.corr_size * 4,
             "texture": clt + T * 40 + (self.TX + 1) * 8 * (self.TY + 1) * 8 * 4 * 4,
         }
@@ -520,7 +542,8 @@ def run_b200(args, rank, world, local, pg):
     torch.cuda.set_device(local)
     from tile_processor_gpu_b200 import build
     build.build()
-    pipe = FramePipeline(seed=100 + rank, device=dev)
+    size = tuple(int(v) for v in args.frame.split("x"))
+    pipe = FramePipeline(seed=100 + rank, device=dev, size=size)
     stream = torch.cuda.current_stream()
     # launch shapes (grid caps) of the three stage kernels, tuned on this frame
     from tile_processor_gpu_b200 import autotune
@@ -606,6 +629,33 @@ def run_b200(args, rank, world, local, pg):
     except Exception as e:  # capture is optional: the eager step is the measurement
         graph_ms = "capture failed: %s" % str(e).splitlines()[0][:120]
 
+    # the precision form (tensor-core transforms), both operand formats
+    precision = {}
+    for name, fmt in (("fp16x2", pipe.api.TC_FP16X2), ("bf16x2", pipe.api.TC_BF16X2)):
+        try:
+            for _ in range(2):
+                for st in pipe.STAGES:
+                    pipe.precision_stage(st, fmt)
+            torch.cuda.synchronize()
+            evp = {st: [] for st in pipe.STAGES}
+            for _ in range(fused_steps):
+                for st in pipe.STAGES:
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    pipe.precision_stage(st, fmt)
+                    b.record(stream)
+                    evp[st].append((a, b))
+            torch.cuda.synchronize()
+            pst = {st: sum(a.elapsed_time(b) for a, b in v) / fused_steps for st, v in evp.items()}
+            precision[name] = {"frame_ms": round(sum(pst.values()), 4),
+                               "frames_per_s": round(1e3 / sum(pst.values()), 1),
+                               "stages_ms": {k: round(v, 4) for k, v in pst.items()},
+                               "timed_out": pipe.api.tc_status()}
+        except Exception as e:  # reported beside the plain path, never instead of it
+            precision[name] = {"error": str(e).splitlines()[0][:200]}
+    # leave the plain path's outputs in the buffers for what follows
+    pipe.step()
+
     # the disparity fit on the frame's correlations (the consumer of stage 2)
     pipe.step()
     pipe.disparity_fit()
@@ -645,7 +695,7 @@ def run_b200(args, rank, world, local, pg):
 
     # ---- the batched workload: 64 uneven sparse frames, one CUDA graph ----
     batched = None
-    if not args.no_batched:
+    if not args.no_batched and size == (WIDTH, HEIGHT):
         batch = BatchedFrames(pipe, n=64, seed=11 + rank)
         batch_shapes = None
         if not args.no_tune and not args.shapes:
@@ -718,11 +768,17 @@ def run_b200(args, rank, world, local, pg):
         "metric": METRIC, "value": round(fps, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plane scene, centred PSF kernels)",
-        "config": bench_config(world),
+        "config": bench_config(world) if size == (WIDTH, HEIGHT) else dict(
+            bench_config(world), frame="%dx%d" % size, tiles=pipe.num_tiles, corr_tiles=pipe.num_corr,
+            workload="profiling case (not the benchmark workload)"),
         "frames_per_step": F, "ms_per_frame": round(ms_max / frames_timed, 4),
         "path": "tp_convert_correct_tiles + tp_correlate2D + tp_generate_RBGA",
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "fused_frame_ms": round(fused_ms, 4),
+        "precision": {"what": "the same three calls with each stage's 8x8 transforms as tcgen05 GEMMs "
+                              "(tp_*_tc: split 16-bit operands, three MMAs per product, FP32 accumulation); "
+                              "errors against the FP64 oracle in parity.precision",
+                      **precision},
         "graph_frame_ms": graph_ms,
         "disparity": disparity,
         "batched": batched,
@@ -747,7 +803,7 @@ def run_b200(args, rank, world, local, pg):
 # --------------------------------------------------------------------------- #
 # CPU implementation (the FP64 port of the reference's tile math)
 # --------------------------------------------------------------------------- #
-def cpu_pipeline(sample_tiles, seed=100, size=None):
+def cpu_pipeline(sample_tiles, seed=100, size=None, peak=None):
     """A bounded sample of the workload for the CPU port: a crop of the same
     seeded scene, sized to about `sample_tiles` tiles (or a whole frame of
     `size` = (w, h)), through all three stages (the per-tile work does not
@@ -763,7 +819,8 @@ def cpu_pipeline(sample_tiles, seed=100, size=None):
     if size is not None:
         w, h = size
     geom = synth.geometry(w, h, image_rows=h + 16)
-    imgs, disp = synth.plane_scene(rng, w, h, disparity=(0.0, 64.0), texture="detail")
+    kw = {} if peak is None else {"peak": peak}
+    imgs, disp = synth.plane_scene(rng, w, h, disparity=(0.0, 64.0), texture="detail", **kw)
     dstride = w + 64
     pitched = np.zeros((4, h + 16, dstride), np.float32)
     pitched[:, :h, :w] = imgs
@@ -784,16 +841,13 @@ def cpu_pipeline(sample_tiles, seed=100, size=None):
                 what=("the whole %dx%d frame (%d tiles)" if full else "%dx%d crop (%d tiles)") % (w, h, tasks.size))
 
 
-def sample_parity(S):
-    """This library's three calls on the CPU sample's inputs, checked against
-    the FP64 oracle: the CLT from the same inputs, the correlations and the
-    overlapped RGBA image from this library's CLT (the tests' rule: texture
-    pixels on stable outputs only, oracle/conditioning.py).  Relative to the
-    oracle's largest magnitude per array / per RGBA slice."""
+def _gpu_on_sample(S, fmt=None):
+    """This library's three calls on a CPU sample's inputs (fmt None: the
+    plain path; else the precision form with that operand format): CLT,
+    correlations, RGBA image and window as host arrays."""
     import torch
-    import conditioning
     from tile_processor_gpu_b200 import api
-    O, geom, TX, TY = S["O"], S["geom"], S["TX"], S["TY"]
+    geom, TX, TY = S["geom"], S["TX"], S["TY"]
     dev = "cuda"
     pa = api.PointerArray
     g = api.Geometry.from_dict(geom)
@@ -803,44 +857,110 @@ def sample_parity(S):
     tasks = api.tasks_to_device(S["tasks"], dev)
     n, idx = S["ntiles"], S["corr_idx"]
     clt = [torch.zeros(TX * TY * 768, dtype=torch.float32, device=dev) for _ in range(4)]
-    api.convert_correct_tiles(g, pa(extras), pa(kernels), pa(images), tasks, pa(clt), S["dstride"], n, 0)
     corrs = torch.zeros((len(idx), 225), dtype=torch.float32, device=dev)
-    api.correlate2D(g, pa(clt), 3, .25, .25, .5, FAT_ZERO, len(idx), torch.from_numpy(idx).to(dev), 225,
-                    CORR_RADIUS, corrs)
+    idx_d = torch.from_numpy(idx).to(dev)
     stride, rows = (TX + 1) * 8, (TY + 1) * 8 * 4
     rgba = torch.zeros((rows, stride), dtype=torch.float32, device=dev)
     lst = torch.zeros(TX * S["TYA"], dtype=torch.int32, device=dev)
     cnt = torch.zeros(8, dtype=torch.int32, device=dev)
     woi_d = torch.zeros(4, dtype=torch.int32, device=dev)
     t = TEXTURE
-    po = np.ascontiguousarray(S["port_offsets"], np.float32).reshape(-1)
-    api.generate_RBGA(g, tasks, n, lst, cnt, woi_d, TX, TY, pa(clt), torch.from_numpy(po).to(dev), t["colors"],
-                      t["is_lwir"], t["min_shot"], t["scale_shot"], t["diff_sigma"], t["diff_threshold"],
-                      t["min_agree"], t["weight0"], t["weight1"], t["weight2"], t["dust_remove"], 0, stride, rgba)
+    po = torch.from_numpy(np.ascontiguousarray(S["port_offsets"], np.float32).reshape(-1)).to(dev)
+    targs = (t["colors"], t["is_lwir"], t["min_shot"], t["scale_shot"], t["diff_sigma"], t["diff_threshold"],
+             t["min_agree"], t["weight0"], t["weight1"], t["weight2"], t["dust_remove"], 0, stride, rgba)
+    if fmt is None:
+        api.convert_correct_tiles(g, pa(extras), pa(kernels), pa(images), tasks, pa(clt), S["dstride"], n, 0)
+        api.correlate2D(g, pa(clt), 3, .25, .25, .5, FAT_ZERO, len(idx), idx_d, 225, CORR_RADIUS, corrs)
+        api.generate_RBGA(g, tasks, n, lst, cnt, woi_d, TX, TY, pa(clt), po, *targs)
+    else:
+        tiles = [torch.zeros_like(c) for c in clt]
+        api.convert_correct_tiles_tc(g, pa(extras), pa(kernels), pa(images), tasks, pa(clt), S["dstride"], n, 0,
+                                     fmt=fmt)
+        api.correlate2D_tc(g, pa(clt), 3, .25, .25, .5, FAT_ZERO, len(idx), idx_d, 225, CORR_RADIUS, corrs, fmt=fmt)
+        api.generate_RBGA_tc(g, tasks, n, lst, cnt, woi_d, TX, TY, pa(clt), po, *targs, pa(tiles), fmt=fmt)
     torch.cuda.synchronize()
-    clt_h = [c.cpu().numpy() for c in clt]
-    rel = lambda a, b: float(np.abs(np.asarray(a, np.float64) - b).max() / max(np.abs(b).max(), 1e-300))
-    want = O.convert_correct_tiles(geom, S["extra"], S["kern"], S["pitched"], S["dstride"], S["tasks"])
-    e_clt = max(rel(clt_h[c], want[c]) for c in range(4))
-    c64 = [x.astype(np.float64) for x in clt_h]
-    co = O.correlate2D(geom, c64, 3, .25, .25, .5, FAT_ZERO, idx, 225, CORR_RADIUS)
-    e_corr = rel(corrs.cpu().numpy(), co)
-    o, _, _, _, _ = O.generate_RBGA(geom, S["tasks"], TX, TY, clt_h, po, stride, rows + 8)
-    woi = woi_d.cpu().numpy()
+    return [c.cpu().numpy() for c in clt], corrs.cpu().numpy(), rgba.cpu().numpy(), woi_d.cpu().numpy()
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _rms(a, b):
+    a = np.asarray(a, np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.abs(b).max(), 1e-300))
+
+
+def _rgba_errors(S, rgba, clt_ref, woi):
+    """per-slice errors of an RGBA image against the oracle's from clt_ref,
+    on pixels whose tiles the oracle's conditioning probe finds stable"""
+    import conditioning
+    O, geom, TX, TY = S["O"], S["geom"], S["TX"], S["TY"]
+    po = np.ascontiguousarray(S["port_offsets"], np.float32).reshape(-1)
+    o, _, _, _, woi_o = O.generate_RBGA(geom, S["tasks"], TX, TY, clt_ref, po, rgba.shape[1], rgba.shape[0] + 8)
     h, w = (woi[3] + 1) * 8, (woi[2] + 1) * 8
     txy = S["tasks"]["txy"].astype(np.int64)
     tiles = (txy & 0xFFFF) + (txy >> 16) * TX
-    bad, _ = conditioning.unstable_tiles(O, geom, po, clt_h, tiles)
+    bad, _ = conditioning.unstable_tiles(O, geom, po, clt_ref, tiles)
     m = conditioning.unstable_image_mask(bad.any(axis=1), tiles << 8, woi, TX, (h, w), 4)
     sl = lambda a: a[:4 * h, :w].reshape(4, h, w)[None]
-    per = conditioning.stable_errors(sl(rgba.cpu().numpy()), sl(o), sl(~m))
-    names = ("r", "b", "g", "alpha")
-    return {"against": "FP64 oracle (CPU restatement of the reference's tile math)", "sample": S["what"],
-            "clt_max_rel": float("%.3g" % e_clt), "corr_max_rel": float("%.3g" % e_corr),
-            "texture": {"rule": "overlapped RGBA on pixels whose tiles the oracle's conditioning probe finds stable "
-                                "(1e-6 input perturbations, 6-digit window tables); error relative to the slice "
-                                "maximum",
-                        "slices": {nm: {k: float("%.3g" % v) for k, v in r.items()} for nm, r in zip(names, per)}}}
+    per = conditioning.stable_errors(sl(rgba), sl(o), sl(~m))
+    out = {}
+    for nm, r, k in zip(("r", "b", "g", "alpha"), per, range(4)):
+        keep = ~m[:h]  # the mask is the same for the four slices
+        g_, o_ = sl(rgba)[0, k][keep].astype(np.float64), sl(o)[0, k][keep]
+        r["rms"] = float(np.sqrt(np.mean((g_ - o_) ** 2)) / max(np.abs(o_).max(), 1e-300))
+        out[nm] = {kk: float("%.3g" % v) for kk, v in r.items()}
+    return out, bool(np.array_equal(woi, woi_o))
+
+
+def sample_parity(S, hdr=None):
+    """This library on the CPU sample's inputs, checked against the FP64
+    oracle (the checker).  Plain path: the CLT from the same inputs, the
+    correlations and the overlapped RGBA image from this library's CLT
+    (isolating each stage).  Precision form (both operand formats): each
+    stage fed by the one before it, against the oracle's own pipeline from the
+    same inputs.  Texture pixels are compared where the oracle's conditioning
+    probe finds them stable (1e-6 input perturbations, 6-digit window tables).
+    Errors relative to the oracle's largest magnitude (per RGBA slice).  `hdr`:
+    a second, high-dynamic-range sample run the same way."""
+    O, geom = S["O"], S["geom"]
+    want = O.convert_correct_tiles(geom, S["extra"], S["kern"], S["pitched"], S["dstride"], S["tasks"])
+    idx = S["corr_idx"]
+
+    def plain_record(T):
+        clt, corrs, rgba, woi = _gpu_on_sample(T)
+        w = want if T is S else O.convert_correct_tiles(T["geom"], T["extra"], T["kern"], T["pitched"],
+                                                        T["dstride"], T["tasks"])
+        co = T["O"].correlate2D(T["geom"], [x.astype(np.float64) for x in clt], 3, .25, .25, .5, FAT_ZERO,
+                                T["corr_idx"], 225, CORR_RADIUS)
+        tex, woi_ok = _rgba_errors(T, rgba, clt, woi)
+        return {"sample": T["what"], "clt_max_rel": float("%.3g" % max(_rel(clt[c], w[c]) for c in range(4))),
+                "corr_max_rel": float("%.3g" % _rel(corrs, co)), "window_equal": woi_ok, "texture": tex}, w
+
+    def precision_record(T, w):
+        out = {}
+        from tile_processor_gpu_b200 import api
+        co = T["O"].correlate2D(T["geom"], w, 3, .25, .25, .5, FAT_ZERO, T["corr_idx"], 225, CORR_RADIUS)
+        for name, fmt in (("fp16x2", api.TC_FP16X2), ("bf16x2", api.TC_BF16X2)):
+            clt, corrs, rgba, woi = _gpu_on_sample(T, fmt)
+            tex, woi_ok = _rgba_errors(T, rgba, w, woi)
+            out[name] = {"clt": {"max": float("%.3g" % max(_rel(clt[c], w[c]) for c in range(4))),
+                                 "rms": float("%.3g" % max(_rms(clt[c], w[c]) for c in range(4)))},
+                         "corr": {"max": float("%.3g" % _rel(corrs, co)), "rms": float("%.3g" % _rms(corrs, co))},
+                         "texture": tex, "window_equal": woi_ok}
+        return out
+
+    rec, w = plain_record(S)
+    out = {"against": "FP64 oracle (CPU restatement of the reference's tile math)",
+           "rule": "texture: overlapped RGBA on pixels whose tiles the oracle's conditioning probe finds stable; "
+                   "errors relative to the oracle's largest magnitude (per slice)",
+           **rec, "precision": {"sample": S["what"], **precision_record(S, w)}}
+    if hdr is not None:
+        rh, wh = plain_record(hdr)
+        out["hdr"] = {**rh, "precision": precision_record(hdr, wh)}
+    return out
 
 
 def cpu_baseline(sample_tiles, min_seconds=10.0, max_reps=5):
@@ -869,7 +989,8 @@ def cpu_baseline(sample_tiles, min_seconds=10.0, max_reps=5):
            "full_frame_ms": round(1e3 * dt / frames, 1), "small_256x256_ms": round(small_ms, 2)}
     parity = None
     try:
-        parity = sample_parity(S)
+        hdr = cpu_pipeline(0, size=(1024, 768), peak=1e4, seed=31)
+        parity = sample_parity(S, hdr=hdr)
     except Exception as e:  # the record is informative; the GPU tests are the parity gate
         parity = {"error": str(e).splitlines()[0][:200]}
     return rec, parity
@@ -997,6 +1118,8 @@ def main():
     ap.add_argument("--no-reference-kernels", action="store_true",
                     help="reference arm: skip the rebuilt reference kernels' GPU timing")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-frame batched workload")
+    ap.add_argument("--frame", default="%dx%d" % (WIDTH, HEIGHT),
+                    help="frame size WxH of the main workload (other sizes for profiling captures only)")
     ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes instead of tuned ones")
     ap.add_argument("--shapes", default="", help="fixed launch shapes, e.g. convert=8,correlate=6,textures=4")
     args = ap.parse_args()
