@@ -692,6 +692,14 @@ def run_b200(args, rank, world, local, pg):
         # algorithmic work of one inference: 2 (1350*256 + 256*128 + 128*2) flops and the 1350 FP32 features per row
         disparity["learned"]["infer_tflops"] = round(rows * 2 * (1350 * 256 + 256 * 128 + 128 * 2) / infer_ms / 1e9, 1)
         disparity["learned"]["infer_feature_gbs"] = round(rows * 1350 * 4 / infer_ms / 1e6, 1)
+        # what each estimate costs the frame: the stage kernels plus the plain
+        # fit, and plus the features and the inference for the learned one
+        frame_ms = ms / frames_timed
+        learned_ms = fit_ms + disparity["learned"]["features_ms"] + infer_ms
+        disparity["per_frame_cost"] = {
+            "plain_fit_ms": round(fit_ms, 4), "learned_ms": round(learned_ms, 4),
+            "frames_per_s_with_plain_fit": round(1e3 / (frame_ms + fit_ms), 1),
+            "frames_per_s_with_learned": round(1e3 / (frame_ms + learned_ms), 1)}
 
     # ---- the batched workload: 64 uneven sparse frames, one CUDA graph ----
     batched = None

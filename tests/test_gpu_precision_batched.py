@@ -177,6 +177,10 @@ def test_bench_batched_frames_vs_oracle(native, oracle):
     records = {}
     for k in pick:
         f = fs[k]
+        # the CLT buffer is shared by the batch: tiles this frame does not
+        # list would keep an earlier frame's coefficients
+        for c in pipe.clt:
+            c.zero_()
         batch.run_frame(f)
         torch.cuda.synchronize()
         geom, TX, TY = f["geom"], f["TX"], f["TY"]
