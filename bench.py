@@ -536,6 +536,69 @@ class FramePipeline:
         }
 
 
+def run_child(child_args, timeout):
+    """bench.py --child ... in a subprocess; its last stdout line as JSON (or
+    the reason there is none)"""
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--child"] + child_args
+    try:
+        res = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": "child %s: no result within %d s" % (child_args[0], timeout)}
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+    if res.returncode != 0 or not lines:
+        tail = (res.stderr.strip().splitlines() or ["(no output)"])[-1][:200]
+        return {"error": "child %s exited %d: %s" % (child_args[0], res.returncode, tail)}
+    return json.loads(lines[-1])
+
+
+def child_precision_timing(args):
+    """The precision form (tp_*_tc) on the bench frame, both operand formats:
+    per-stage CUDA-event times over `args.steps` frames after two warm-up
+    frames."""
+    import torch
+    size = tuple(int(v) for v in args.frame.split("x"))
+    pipe = FramePipeline(seed=100, device="cuda:0", size=size)
+    stream = torch.cuda.current_stream()
+    pipe.step()
+    torch.cuda.synchronize()
+    precision = {}
+    for name, fmt in (("fp16x2", pipe.api.TC_FP16X2), ("bf16x2", pipe.api.TC_BF16X2)):
+        try:
+            for _ in range(2):
+                for st in pipe.STAGES:
+                    pipe.precision_stage(st, fmt)
+            torch.cuda.synchronize()
+            evp = {st: [] for st in pipe.STAGES}
+            for _ in range(args.steps):
+                for st in pipe.STAGES:
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    pipe.precision_stage(st, fmt)
+                    b.record(stream)
+                    evp[st].append((a, b))
+            torch.cuda.synchronize()
+            pst = {st: sum(a.elapsed_time(b) for a, b in v) / args.steps for st, v in evp.items()}
+            precision[name] = {"frame_ms": round(sum(pst.values()), 4),
+                               "frames_per_s": round(1e3 / sum(pst.values()), 1),
+                               "stages_ms": {k: round(v, 4) for k, v in pst.items()},
+                               "timed_out": pipe.api.tc_status()}
+        except Exception as e:  # reported beside the plain path, never instead of it
+            precision[name] = {"error": str(e).splitlines()[0][:200]}
+    return precision
+
+
+def child_precision_parity(args):
+    """The precision form's per-stage errors against the FP64 oracle on the
+    CPU-baseline sample and on the HDR scene (the checker; see sample_parity)"""
+    S = cpu_pipeline(args.cpu_sample_tiles)
+    hdr = cpu_pipeline(0, size=(1024, 768), peak=1e4, seed=31)
+    out = {}
+    for name, T in (("sample", S), ("hdr", hdr)):
+        w = T["O"].convert_correct_tiles(T["geom"], T["extra"], T["kern"], T["pitched"], T["dstride"], T["tasks"])
+        out[name] = {"sample": T["what"], **precision_errors(T, w)}
+    return out
+
+
 def run_b200(args, rank, world, local, pg):
     import torch
     dev = "cuda:%d" % local
@@ -629,32 +692,10 @@ def run_b200(args, rank, world, local, pg):
     except Exception as e:  # capture is optional: the eager step is the measurement
         graph_ms = "capture failed: %s" % str(e).splitlines()[0][:120]
 
-    # the precision form (tensor-core transforms), both operand formats
-    precision = {}
-    for name, fmt in (("fp16x2", pipe.api.TC_FP16X2), ("bf16x2", pipe.api.TC_BF16X2)):
-        try:
-            for _ in range(2):
-                for st in pipe.STAGES:
-                    pipe.precision_stage(st, fmt)
-            torch.cuda.synchronize()
-            evp = {st: [] for st in pipe.STAGES}
-            for _ in range(fused_steps):
-                for st in pipe.STAGES:
-                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    a.record(stream)
-                    pipe.precision_stage(st, fmt)
-                    b.record(stream)
-                    evp[st].append((a, b))
-            torch.cuda.synchronize()
-            pst = {st: sum(a.elapsed_time(b) for a, b in v) / fused_steps for st, v in evp.items()}
-            precision[name] = {"frame_ms": round(sum(pst.values()), 4),
-                               "frames_per_s": round(1e3 / sum(pst.values()), 1),
-                               "stages_ms": {k: round(v, 4) for k, v in pst.items()},
-                               "timed_out": pipe.api.tc_status()}
-        except Exception as e:  # reported beside the plain path, never instead of it
-            precision[name] = {"error": str(e).splitlines()[0][:200]}
-    # leave the plain path's outputs in the buffers for what follows
-    pipe.step()
+    # the precision form (tensor-core transforms), both operand formats, timed
+    # in a child process on its own copy of the frame: whatever happens there
+    # cannot cost this line
+    precision = run_child(["precision-timing", "--frame", args.frame, "--steps", str(fused_steps)], timeout=900)
 
     # the disparity fit on the frame's correlations (the consumer of stage 2)
     pipe.step()
@@ -923,6 +964,22 @@ def _rgba_errors(S, rgba, clt_ref, woi):
     return out, bool(np.array_equal(woi, woi_o))
 
 
+def precision_errors(T, w):
+    """per-stage errors of the precision form (both formats) on sample T
+    against the oracle pipeline from the same inputs (w: the oracle's CLT)"""
+    from tile_processor_gpu_b200 import api
+    out = {}
+    co = T["O"].correlate2D(T["geom"], w, 3, .25, .25, .5, FAT_ZERO, T["corr_idx"], 225, CORR_RADIUS)
+    for name, fmt in (("fp16x2", api.TC_FP16X2), ("bf16x2", api.TC_BF16X2)):
+        clt, corrs, rgba, woi = _gpu_on_sample(T, fmt)
+        tex, woi_ok = _rgba_errors(T, rgba, w, woi)
+        out[name] = {"clt": {"max": float("%.3g" % max(_rel(clt[c], w[c]) for c in range(4))),
+                             "rms": float("%.3g" % max(_rms(clt[c], w[c]) for c in range(4)))},
+                     "corr": {"max": float("%.3g" % _rel(corrs, co)), "rms": float("%.3g" % _rms(corrs, co))},
+                     "texture": tex, "window_equal": woi_ok, "timed_out": api.tc_status()}
+    return out
+
+
 def sample_parity(S, hdr=None):
     """This library on the CPU sample's inputs, checked against the FP64
     oracle (the checker).  Plain path: the CLT from the same inputs, the
@@ -947,27 +1004,15 @@ def sample_parity(S, hdr=None):
         return {"sample": T["what"], "clt_max_rel": float("%.3g" % max(_rel(clt[c], w[c]) for c in range(4))),
                 "corr_max_rel": float("%.3g" % _rel(corrs, co)), "window_equal": woi_ok, "texture": tex}, w
 
-    def precision_record(T, w):
-        out = {}
-        from tile_processor_gpu_b200 import api
-        co = T["O"].correlate2D(T["geom"], w, 3, .25, .25, .5, FAT_ZERO, T["corr_idx"], 225, CORR_RADIUS)
-        for name, fmt in (("fp16x2", api.TC_FP16X2), ("bf16x2", api.TC_BF16X2)):
-            clt, corrs, rgba, woi = _gpu_on_sample(T, fmt)
-            tex, woi_ok = _rgba_errors(T, rgba, w, woi)
-            out[name] = {"clt": {"max": float("%.3g" % max(_rel(clt[c], w[c]) for c in range(4))),
-                                 "rms": float("%.3g" % max(_rms(clt[c], w[c]) for c in range(4)))},
-                         "corr": {"max": float("%.3g" % _rel(corrs, co)), "rms": float("%.3g" % _rms(corrs, co))},
-                         "texture": tex, "window_equal": woi_ok}
-        return out
-
-    rec, w = plain_record(S)
+    rec, _ = plain_record(S)
     out = {"against": "FP64 oracle (CPU restatement of the reference's tile math)",
            "rule": "texture: overlapped RGBA on pixels whose tiles the oracle's conditioning probe finds stable; "
-                   "errors relative to the oracle's largest magnitude (per slice)",
-           **rec, "precision": {"sample": S["what"], **precision_record(S, w)}}
+                   "errors relative to the oracle's largest magnitude (per slice)", **rec}
     if hdr is not None:
-        rh, wh = plain_record(hdr)
-        out["hdr"] = {**rh, "precision": precision_record(hdr, wh)}
+        out["hdr"], _ = plain_record(hdr)
+    # the precision form, per stage, each fed by the one before it, against
+    # the oracle's own pipeline (in a child process: see run_child)
+    out["precision"] = run_child(["precision-parity", "--cpu-sample-tiles", str(S["ntiles"])], timeout=900)
     return out
 
 
@@ -1130,7 +1175,13 @@ def main():
                     help="frame size WxH of the main workload (other sizes for profiling captures only)")
     ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes instead of tuned ones")
     ap.add_argument("--shapes", default="", help="fixed launch shapes, e.g. convert=8,correlate=6,textures=4")
+    ap.add_argument("--child", default="", choices=["", "precision-timing", "precision-parity"],
+                    help="internal: one measurement in a subprocess of the main arm")
     args = ap.parse_args()
+    if args.child:
+        fn = child_precision_timing if args.child == "precision-timing" else child_precision_parity
+        print(json.dumps(fn(args)))
+        return
     if args.impl == "reference":
         # CPU arm: rank 0 alone runs it, the other ranks exit without work
         rank = int(os.environ.get("RANK", "0"))

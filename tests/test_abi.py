@@ -148,3 +148,18 @@ def test_zero_work_is_ok_without_gpu(native):
     assert N.call("tp_disparity_fit", g.ptr, None, 225, 7, 0, None, None, 63, 0, None, None, None) == 0
     assert N.call("tp_textures_accumulate", g.ptr, None, fake, 0, None, None, 3, 0, 10., 3., 1.5, 10., 3., .3, .1, .6, 1,
                   0, 0, None, 0, None, None) == 0
+
+
+def test_library_never_ends_the_process(native):
+    """Errors come back as status codes: the library imports no function that
+    ends the caller's process (a device-only helper called from host code
+    compiles to such a call)."""
+    import shutil
+    import subprocess
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm not available")
+    from tile_processor_gpu_b200 import _native
+    out = subprocess.run([nm, "-D", "--undefined-only", _native.LIB_PATH], capture_output=True, text=True).stdout
+    names = {ln.split()[-1].split("@")[0] for ln in out.splitlines() if ln.strip()}
+    assert not names & {"exit", "_exit", "_Exit", "abort", "quick_exit"}, sorted(names & {"exit", "_exit", "abort"})

@@ -101,7 +101,7 @@ struct CorrTcStage {
     float *corrs;
     float up; /* FP16 row scale (a power of two); 1 for BF16 */
 
-    __device__ __forceinline__ long long rows() const { return num; }
+    __host__ __device__ __forceinline__ long long rows() const { return num; }
 
     __device__ __forceinline__ int entry(long long n, int *tile, int *pair) const
     {

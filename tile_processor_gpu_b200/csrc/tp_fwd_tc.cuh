@@ -46,7 +46,7 @@ struct FwdTcStage {
     int num_tiles;
     int lpf_mask;
 
-    __device__ __forceinline__ long long rows() const { return 12LL * num_tiles; }
+    __host__ __device__ __forceinline__ long long rows() const { return 12LL * num_tiles; }
 
     /* task, camera and colour of row n; the tile (or -1) */
     __device__ __forceinline__ int job(long long n, int *cam, int *color, float *cx, float *cy) const

@@ -43,7 +43,7 @@ struct InvTcStage {
     const int *list;     /* NULL: tasks mode                                 */
     int colors;
 
-    __device__ __forceinline__ long long rows() const { return 12 * num; }
+    __host__ __device__ __forceinline__ long long rows() const { return 12 * num; }
 
     /* the job of row n: tile (or -1), camera and colour */
     __device__ __forceinline__ int job(long long n, int *cam, int *color) const
