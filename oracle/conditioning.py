@@ -45,14 +45,16 @@ def texture_outputs(oracle, case, clt64, idx, keep_weights=0, colors=3):
     return out.reshape(len(idx), ns, 16, 16)
 
 
-def unstable_mask(oracle, case, clt64, idx, keep_weights=0, colors=3, trials=8, seed=100):
-    """(unstable [n][ns][16][16] bool per slice, oracle outputs [n][ns][16][16])"""
+def unstable_mask(oracle, case, clt64, idx, keep_weights=0, colors=3, trials=8, seed=100, eps=EPS):
+    """(unstable [n][ns][16][16] bool per slice, oracle outputs [n][ns][16][16]);
+    eps: the relative size of the input perturbations (the probed path's own
+    error level; 1e-6 for float32 evaluations)"""
     base = texture_outputs(oracle, case, clt64, idx, keep_weights, colors)
     scale = np.maximum(np.abs(base).max(axis=(0, 2, 3)), 1e-300)[None, :, None, None]
     bad = np.zeros(base.shape, dtype=bool)
     for t in range(trials):
         rng = np.random.default_rng(seed + t)
-        pert = [c * (1.0 + EPS * rng.standard_normal(c.shape)) for c in clt64]
+        pert = [c * (1.0 + eps * rng.standard_normal(c.shape)) for c in clt64]
         o = texture_outputs(oracle, case, pert, idx, keep_weights, colors)
         bad |= np.abs(o - base) / scale > TOL
     oracle.set_table_mode(1)
@@ -88,7 +90,7 @@ class _Frame:
         self.port_offsets = port_offsets
 
 
-def unstable_tiles(oracle, geom, port_offsets, clt, tiles, keep_weights=0, colors=3, chunk=8192, trials=8):
+def unstable_tiles(oracle, geom, port_offsets, clt, tiles, keep_weights=0, colors=3, chunk=8192, trials=8, eps=EPS):
     """unstable_mask for the tiles `tiles` (tile numbers) of a large frame,
     in chunks, so host memory stays bounded: each chunk's CLT is gathered into
     compact FP64 arrays and its tiles renumbered 0..n-1 (the per-tile outputs
@@ -102,7 +104,7 @@ def unstable_tiles(oracle, geom, port_offsets, clt, tiles, keep_weights=0, color
         t = tiles[a:a + chunk]
         sub = [np.asarray(c, dtype=np.float32).reshape(-1, 768)[t].astype(np.float64).reshape(-1) for c in clt]
         idx = ((np.arange(t.size, dtype=np.int64) << 8) | 0x80 | 0xF).astype(np.int32)
-        b, o = unstable_mask(oracle, fr, sub, idx, keep_weights, colors, trials=trials)
+        b, o = unstable_mask(oracle, fr, sub, idx, keep_weights, colors, trials=trials, eps=eps)
         bads.append(b)
         bases.append(o)
     return np.concatenate(bads), np.concatenate(bases)

@@ -326,7 +326,7 @@ def _rgba_region(woi, colors=3):
     return h, w
 
 
-def _rgba_stable(oracle, fr, clt64, woi):
+def _rgba_stable(oracle, fr, clt64, woi, eps=1e-6):
     """stable pixels of the overlapped RGBA image (all four slices)"""
     import conditioning
     c = fr.case
@@ -338,7 +338,7 @@ def _rgba_stable(oracle, fr, clt64, woi):
         entries += idx[q * quarter: q * quarter + counts[2 * q]].tolist()
         entries += idx[(q + 1) * quarter - counts[2 * q + 1]: (q + 1) * quarter].tolist()
     entries = np.array(entries, dtype=np.int32)
-    bad, _ = conditioning.unstable_mask(oracle, c, clt64, entries, 0)
+    bad, _ = conditioning.unstable_mask(oracle, c, clt64, entries, 0, eps=eps)
     h, w = _rgba_region(woi)
     m = conditioning.unstable_image_mask(bad.any(axis=1), entries, woi, c.TX, (h, w), 4)
     assert m.mean() <= MAX_UNSTABLE_COLOR
