@@ -326,7 +326,7 @@ def _rgba_region(woi, colors=3):
     return h, w
 
 
-def _rgba_stable(oracle, fr, clt64, woi, eps=1e-6):
+def _rgba_stable(oracle, fr, clt64, woi, eps=1e-6, max_unstable=MAX_UNSTABLE_COLOR):
     """stable pixels of the overlapped RGBA image (all four slices)"""
     import conditioning
     c = fr.case
@@ -341,7 +341,7 @@ def _rgba_stable(oracle, fr, clt64, woi, eps=1e-6):
     bad, _ = conditioning.unstable_mask(oracle, c, clt64, entries, 0, eps=eps)
     h, w = _rgba_region(woi)
     m = conditioning.unstable_image_mask(bad.any(axis=1), entries, woi, c.TX, (h, w), 4)
-    assert m.mean() <= MAX_UNSTABLE_COLOR
+    assert m.mean() <= max_unstable
     return ~m
 
 

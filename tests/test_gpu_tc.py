@@ -162,7 +162,9 @@ def test_generate_rbga_tc(frames, oracle, impl, name):
     o, _, _, _, woi_o = oracle.generate_RBGA(c.geom, c.tasks, c.TX, c.TY, clt, c.port_offsets, stride, rows + 8)
     assert np.array_equal(woi, woi_o)
     h, w = (woi[3] + 1) * 8, (woi[2] + 1) * 8
-    keep = _rgba_stable(oracle, fr, [x.astype(np.float64) for x in clt], woi, eps=PROBE_EPS[impl])
+    # at the BF16 probe size more of an HDR frame's pixels are near a tie
+    keep = _rgba_stable(oracle, fr, [x.astype(np.float64) for x in clt], woi, eps=PROBE_EPS[impl],
+                        max_unstable=0.01 if impl == "tc_fp16" else 0.05)
     sl = lambda a: a[:4 * h, :w].reshape(4, h, w)[None]
     rec = _stable_check(sl(b), sl(o), sl(keep), BOUND[impl], frac=4e-4, hard=1e-3 if impl == "tc_fp16" else 1e-2)
     print("\ngenerate_RBGA %s %s %s" % (impl, name, json.dumps(rec)))

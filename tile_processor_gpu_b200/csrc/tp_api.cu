@@ -1014,7 +1014,7 @@ int tc_launch(const S &st, int format, int stage, bool (*attr)[128], tp_stream_t
     int *err = nullptr;
     int rc;
     if ((rc = tc_tables(format, stage, &btab)) || (rc = tc_err_ptr(&err))) return rc;
-    constexpr int smem = tp::tc_stage_smem(S::kQuads, S::kMeta);
+    constexpr int smem = tp::tc_stage_smem(S::kQuads, S::kMeta, S::kAStages);
     const void *kern = format == TP_TC_BF16X2 ? (const void *)tp::k_tc_stage<S, TP_TC_BF16X2>
                                               : (const void *)tp::k_tc_stage<S, TP_TC_FP16X2>;
     if ((rc = set_smem_once(attr[format], kern, smem, what))) return rc;

@@ -12,7 +12,7 @@
  * quadrants into the (2r+1)^2 output.
  *
  * Runs in the shared pipeline k_tc_stage (tp_tc_engine.cuh) over blocks of
- * 128 index entries: eight producer warps, one 8-lane group per entry,
+ * 128 index entries: twelve producer warps, one 8-lane group per entry,
  * compute row l of the four accumulated quadrants and write them split into
  * the A image; four epilogue warps, one thread per entry, read the
  * pixel-domain quadrants row by row from tensor memory, unfold and store
@@ -84,12 +84,13 @@ __device__ __forceinline__ void corr_product_rows(const float *a, const float *b
 }
 
 /* The correlation as a tensor-core stage (k_tc_stage): rows are index
- * entries; eight producer warps (the CLT products are the heavy part), four
- * epilogue warps. */
+ * entries; twelve producer warps (the CLT products are the heavy part), four
+ * epilogue warps (512 threads, at most 128 registers each). */
 struct CorrTcStage {
-    static constexpr int kQuads = 4, kProdWarps = 8, kEpiWarps = 4;
+    static constexpr int kQuads = 4, kProdWarps = 12, kEpiWarps = 4;
     static constexpr int kThreads = 32 * (kProdWarps + kEpiWarps);
     static constexpr int kMeta = 1;
+    static constexpr int kAStages = 1;
     Geom g;
     float *const *clt;
     int colors;

@@ -33,9 +33,10 @@
 namespace tp {
 
 struct FwdTcStage {
-    static constexpr int kQuads = 2, kProdWarps = 4, kEpiWarps = 8;
+    static constexpr int kQuads = 2, kProdWarps = 16, kEpiWarps = 8;
     static constexpr int kThreads = 32 * (kProdWarps + kEpiWarps);
     static constexpr int kMeta = 36;
+    static constexpr int kAStages = 2; /* two slots: two A images fit */
     Geom g;
     size_t dstride;
     float *const *kernel_offsets;

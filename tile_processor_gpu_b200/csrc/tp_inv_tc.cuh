@@ -32,9 +32,10 @@
 namespace tp {
 
 struct InvTcStage {
-    static constexpr int kQuads = 4, kProdWarps = 4, kEpiWarps = 8;
+    static constexpr int kQuads = 4, kProdWarps = 16, kEpiWarps = 8;
     static constexpr int kThreads = 32 * (kProdWarps + kEpiWarps);
     static constexpr int kMeta = 2;
+    static constexpr int kAStages = 1;
     Geom g;
     float *const *clt;   /* in: per camera [tiles][3][256]                  */
     float *const *tiles; /* out: per camera [tiles][3][16][16]              */

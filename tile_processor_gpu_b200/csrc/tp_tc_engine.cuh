@@ -24,8 +24,10 @@
  * descriptor's start by 32 bytes inside the swizzle atom.
  *
  * k_tc_stage<S, FMT> is the pipeline every stage shares; S supplies the
- * work (rows, producer, epilogue).  Persistent, one CTA per SM, blocks of
- * 128 rows (jobs):
+ * work (rows, producer, epilogue).  Persistent, one CTA per SM (512 or 768
+ * threads: the producers' loads and the epilogues' per-job work are latency
+ * bound, so the stages take as many warps as their registers allow), blocks
+ * of 128 rows (jobs):
  *   producer warps: one 8-lane group per row writes its quadrants, split,
  *     into the A image and (lane 0) the row's metadata words; after a named
  *     barrier thread 0 issues the block's 12 Q MMAs into accumulator buffer
@@ -35,9 +37,12 @@
  *     epilogue warps, warps e and e + 4 share the rows and split the work:
  *     part e / 4); it waits for meta[block & 1] and mma[block & 1], runs
  *     S::epilogue, and the warp then releases the buffer (free[block & 1]).
- * Before the producers fill block b, thread 0 waits for the MMAs of block b-1
- * (the A image is free) and for the epilogue of block b-2 (its accumulator
- * and metadata buffer are free), and publishes the outcome before a named
+ * Before the producers fill block b, thread 0 waits for the epilogue of
+ * block b-2 (its accumulator and metadata buffer are free) and, with one A
+ * image, for the MMAs of block b-1 (the A image is free; a stage with two
+ * quadrant slots keeps two A images, block b filling image b % 2, whose last
+ * reader, block b-2's MMAs, completed before that block's epilogue ran), and
+ * publishes the outcome before a named
  * barrier, so all producer threads go on or leave together; each epilogue
  * warp agrees on its waits with a vote.  The metadata reach the epilogue
  * through the meta mbarrier's release / acquire.  Every wait is bounded: one
@@ -180,11 +185,11 @@ __device__ __forceinline__ void tc_producer_sync(int nthreads)
     asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 
-/* dynamic shared memory of k_tc_stage for a stage of Q quadrants and M
- * metadata words per row */
-__host__ __device__ constexpr int tc_stage_smem(int Q, int M)
+/* dynamic shared memory of k_tc_stage for a stage of Q quadrants, M
+ * metadata words per row and AS A images */
+__host__ __device__ constexpr int tc_stage_smem(int Q, int M, int AS)
 {
-    return 1024 + 2 * Q * kTcQuadBytes + 2 * Q * kTcBQuadBytes + 2 * kTcRows * M * 4 + 8 * 8 + 32;
+    return 1024 + AS * 2 * Q * kTcQuadBytes + 2 * Q * kTcBQuadBytes + 2 * kTcRows * M * 4 + 8 * 8 + 32;
 }
 
 template <class S, int FMT>
@@ -194,7 +199,9 @@ __global__ void __launch_bounds__(S::kThreads, 1) k_tc_stage(const S st, const u
     constexpr int Q = S::kQuads;
     constexpr int kMetaWords = S::kMeta;
     constexpr int kProd = 32 * S::kProdWarps;
-    constexpr int kABytes = 2 * Q * kTcQuadBytes, kBBytes = 2 * Q * kTcBQuadBytes;
+    constexpr int kAStages = S::kAStages; /* 1, or 2: block b fills A image b % 2 */
+    static_assert(kAStages == 1 || kAStages == 2, "A images");
+    constexpr int kAImage = 2 * Q * kTcQuadBytes, kABytes = kAStages * kAImage, kBBytes = 2 * Q * kTcBQuadBytes;
     constexpr uint32_t kCols = (uint32_t)(2 * 64 * Q); /* 256 or 512 */
     enum { kBarB = 0, kBarMma = 1, kBarMeta = 3, kBarFree = 5, kBarDrain = 7, kBars = 8 };
     extern __shared__ __align__(1024) unsigned char tcs_smem[];
@@ -240,7 +247,6 @@ __global__ void __launch_bounds__(S::kThreads, 1) k_tc_stage(const S st, const u
     int issued = 0;
 
     if (producer) {
-        const TcA<Q> A{sm};
         const int l = tid & 7, grp = tid >> 3;
         const unsigned gm = group_mask();
         if (issuer && blockIdx.x < nblocks) {
@@ -253,8 +259,10 @@ __global__ void __launch_bounds__(S::kThreads, 1) k_tc_stage(const S st, const u
         for (long long blk = blockIdx.x; blk < nblocks; blk += gridDim.x, lb++) {
             if (issuer) {
                 bool ok = !flags[0];
-                /* the A image: free once the previous block's MMAs completed */
-                if (ok && lb > 0)
+                /* one A image: free once the previous block's MMAs completed.  Two:
+                 * image lb % 2 was last read by the MMAs of block lb - 2, which
+                 * completed before that block's epilogue ran (waited for below) */
+                if (kAStages == 1 && ok && lb > 0)
                     ok = tc_wait_or_abort(bar(kBarMma + ((lb - 1) & 1)), (uint32_t)(((lb - 1) >> 1) & 1), flags);
                 /* accumulator and metadata buffer: free once block lb - 2's epilogue released them */
                 if (ok && lb >= 2)
@@ -265,6 +273,7 @@ __global__ void __launch_bounds__(S::kThreads, 1) k_tc_stage(const S st, const u
             tc_producer_sync(kProd);
             if (!flags[1]) break;
             uint32_t *mb = meta + (lb & 1) * kTcRows * kMetaWords;
+            const TcA<Q> A{sm + (lb % kAStages) * kAImage};
 #pragma unroll 1
             for (int row = grp; row < kTcRows; row += kProd / 8)
                 st.template produce<FMT>(blk * kTcRows + row, row, l, gm, A, mb + row * kMetaWords);
@@ -281,8 +290,8 @@ __global__ void __launch_bounds__(S::kThreads, 1) k_tc_stage(const S st, const u
                     flags[0] = 1;
                 } else {
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    tc_issue_block<Q>(tmem + 64u * Q * (uint32_t)(lb & 1), aA, aB,
-                                      tc_idesc(kTcRows, 64, tc_idesc_fmt(FMT)));
+                    tc_issue_block<Q>(tmem + 64u * Q * (uint32_t)(lb & 1), aA + (uint32_t)((lb % kAStages) * kAImage),
+                                      aB, tc_idesc(kTcRows, 64, tc_idesc_fmt(FMT)));
                     tc_commit(bar(kBarMma + (lb & 1)));
                     issued++;
                 }
