@@ -36,7 +36,9 @@ struct FwdTcStage {
     static constexpr int kQuads = 2, kProdWarps = 16, kEpiWarps = 8;
     static constexpr int kThreads = 32 * (kProdWarps + kEpiWarps);
     static constexpr int kMeta = 36;
-    static constexpr int kAStages = 2; /* two slots: two A images fit */
+    /* One A image: a second slot (double buffering) measured 15% slower, the
+     * larger shared-memory carve-out leaving less L1 for the producers' loads. */
+    static constexpr int kAStages = 1;
     Geom g;
     size_t dstride;
     float *const *kernel_offsets;
