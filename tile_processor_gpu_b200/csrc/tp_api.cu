@@ -117,7 +117,7 @@ int shape_per_sm(int which)
  * their attribute once per device (the first call; make it before capturing
  * a stream into a graph). */
 std::mutex g_attr_mutex;
-bool g_tex_attr[128], g_tex_t_attr[128], g_frame_attr[128], g_tc_attr[128];
+bool g_tex_attr[4][128], g_frame_attr[128], g_tc_attr[128];
 
 int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
 {
@@ -135,11 +135,18 @@ int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
 
 int texture_smem_setup()
 {
-    const int rc = set_smem_once(g_tex_attr, (const void *)tp::k_textures<false>, tp::kTexSmemBytes,
-                                 "cudaFuncSetAttribute(k_textures)");
-    if (rc) return rc;
-    return set_smem_once(g_tex_t_attr, (const void *)tp::k_textures<true>, tp::kTexSmemBytes,
-                         "cudaFuncSetAttribute(k_textures<tiles>)");
+    int rc = set_smem_once(g_tex_attr[0], (const void *)tp::k_textures<false, true>, tp::kTexSmemBytes,
+                           "cudaFuncSetAttribute(k_textures)");
+    if (!rc)
+        rc = set_smem_once(g_tex_attr[1], (const void *)tp::k_textures<true, true>, tp::kTexSmemBytes,
+                           "cudaFuncSetAttribute(k_textures<tiles>)");
+    if (!rc)
+        rc = set_smem_once(g_tex_attr[2], (const void *)tp::k_textures<false, false>, tp::kTexSmemBytes,
+                           "cudaFuncSetAttribute(k_textures<RGBA>)");
+    if (!rc)
+        rc = set_smem_once(g_tex_attr[3], (const void *)tp::k_textures<true, false>, tp::kTexSmemBytes,
+                           "cudaFuncSetAttribute(k_textures<tiles, RGBA>)");
+    return rc;
 }
 
 /* Scratch of tp_generate_RBGA_noalloc: [0, 8) sub-list counts, [8, 12) window
@@ -370,7 +377,7 @@ int tp_textures_accumulate(const tp_geometry *g, const int *woi, float *const *c
     if ((rc = sm_count(&sms))) return rc;
     if ((rc = texture_smem_setup())) return rc;
     unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
-    tp::k_textures<false><<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
+    tp::k_textures<false, true><<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
         gd, woi, clt, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
         want_tiles ? texture_tiles : nullptr);
@@ -561,11 +568,11 @@ static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, in
         const int *base = texture_indices + parity * quarter;
         const cudaError_t err =
             format >= 0
-                ? launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures<true>, gd,
+                ? launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures<true, false>, gd,
                                  (const int *)woi, src, 0LL, (const int *)base, (const int *)num_texture_tiles,
                                  parity << 1, quarter, -quarter, port_offsets, p, texture_rbga_stride, texture_tiles,
                                  (size_t)0, (float *)nullptr)
-                : launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures<false>, gd,
+                : launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures<false, false>, gd,
                                  (const int *)woi, src, 0LL, (const int *)base, (const int *)num_texture_tiles,
                                  parity << 1, quarter, -quarter, port_offsets, p, texture_rbga_stride, texture_tiles,
                                  (size_t)0, (float *)nullptr);
@@ -635,9 +642,11 @@ int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *
     int sms;
     if ((rc = sm_count(&sms))) return rc;
     {
+        /* a programmatic dependent of the list's last kernel, as in generate_rbga */
         const int max_rows = (gd.TY + 1) * 8 * 4;
-        tp::k_clear_rbga<<<grid_for(max_rows, 1, sms, 16), 256, 0, s>>>(woi, 3, 0, 0, texture_rbga_stride,
-                                                                         texture_rbga);
+        const cudaError_t err = launch_chained(true, grid_for(max_rows, 1, sms, 16), 256, 0, s, tp::k_clear_rbga,
+                                               (const int *)woi, 3, 0, 0, texture_rbga_stride, texture_rbga);
+        if (err != cudaSuccess) return cuda_status(err, "process_frame clear launch");
     }
     tp::FrameParams fp;
     fp.lpf_mask = lpf_mask;
@@ -649,15 +658,25 @@ int tp_process_frame(const tp_geometry *g, float *const *kernel_offsets, float *
     fp.corr_radius = corr_radius;
     fp.corr_stride = corr_stride;
     fp.tex = tex;
-    /* odd grid: a grid-stride walk over a raster task list then visits both
-     * column parities in every block */
     if ((rc = set_smem_once(g_frame_attr, (const void *)tp::k_frame, tp::kFrameSmemBytes,
                             "cudaFuncSetAttribute(k_frame)")))
         return rc;
-    unsigned grid = grid_for(num_tiles, 4, sms, 3) | 1u;
-    for (int parity = 0; parity < 4; parity++)
-        tp::k_frame<<<grid, 128, tp::kFrameSmemBytes, s>>>(gd, dstride, kernel_offsets, kernels, images, tasks, num_tiles, parity, fp,
-                                         corrs, port_offsets, woi, texture_rbga_stride, texture_rbga, clt);
+    /* one resident wave, odd: a grid-stride walk over a raster task list then
+     * visits both column parities in every block.  Each parity launch is a
+     * programmatic dependent of the launch before it (the clear, or the
+     * previous parity), which it waits for before its first RGBA update; it
+     * releases its own dependent on entry, so a launch starts only after every
+     * earlier one has started and the first only after the clear released it,
+     * which the clear did once the list (and the tasks' neighbour bits it
+     * rewrites) was complete. */
+    const unsigned grid = grid_for(((long long)num_tiles + 3) / 4, 1, sms, tp::kFrameBlocksPerSm) | 1u;
+    for (int parity = 0; parity < 4; parity++) {
+        const cudaError_t err = launch_chained(true, grid, tp::kFrameThreads, tp::kFrameSmemBytes, s, tp::k_frame,
+                                               gd, dstride, kernel_offsets, kernels, images, (const tp_task *)tasks,
+                                               num_tiles, parity, fp, corrs, port_offsets, (const int *)woi,
+                                               texture_rbga_stride, texture_rbga, clt);
+        if (err != cudaSuccess) return cuda_status(err, "process_frame launch");
+    }
     return cuda_status(cudaGetLastError(), "process_frame launch");
 }
 
@@ -1137,7 +1156,7 @@ int tp_textures_accumulate_tc(const tp_geometry *g, const int *woi, float *const
     if ((rc = sm_count(&sms))) return rc;
     if ((rc = texture_smem_setup())) return rc;
     unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
-    tp::k_textures<true><<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
+    tp::k_textures<true, true><<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
         gd, woi, tile_scratch, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
         want_tiles ? texture_tiles : nullptr);

@@ -23,6 +23,18 @@ namespace tp {
  * quadrants), then the (2r+1)^2 output staging; 536 % 32 == 24 */
 constexpr int kCorrBuf = 4 * 72 + 8 + 240;
 
+/* 4 consecutive floats at p (16-byte aligned when al16) */
+__device__ __forceinline__ void load_row4(const float *p, bool al16, float v[4])
+{
+    if (al16) {
+        const float4 x = *reinterpret_cast<const float4 *>(p);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] = p[k];
+    }
+}
+
 /* 8 consecutive floats at p (16-byte aligned when al16) */
 __device__ __forceinline__ void load_row8(const float *p, bool al16, float v[8])
 {
@@ -38,7 +50,11 @@ __device__ __forceinline__ void load_row8(const float *p, bool al16, float v[8])
 /* One (tile, pair) correlation on an 8-lane group.  a, b: the two cameras'
  * CLT of the tile, colour c at a + c * cstride (4 x 64 floats, row stride 8);
  * global or shared.  tb: kCorrBuf floats of this group.  dst: (2r+1)^2
- * floats. */
+ * floats.  KC: coefficients of the held rows loaded at a time (8: all 64
+ * of both tiles' colour at once, as many loads in flight as possible from
+ * global memory; 4: half the registers, for shared-memory sources).  The
+ * arithmetic and its order do not depend on KC. */
+template <int KC = 8>
 __device__ __forceinline__ void corr_job(const float *a, const float *b, int cstride, int colors, float scale0,
                                          float scale1, float scale2, float fat_zero, int r, float *tb,
                                          float *__restrict__ dst, int l, unsigned gm)
@@ -54,25 +70,37 @@ __device__ __forceinline__ void corr_job(const float *a, const float *b, int cst
         for (int k = 0; k < 8; k++) acc[q][k] = 0.0f;
     for (int color = 0; color < colors; color++) {
         const float s = color == 0 ? scale0 : color == 1 ? scale1 : scale2;
-        float A[4][8], B[4][8];
+        static_assert(KC == 8 || KC == 4, "chunk");
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            load_row8(a + color * cstride + q * 64 + l * 8, al16, A[q]);
-            load_row8(b + color * cstride + q * 64 + l * 8, al16, B[q]);
-        }
+        for (int k0 = 0; k0 < 8; k0 += KC) {
+            float A[4][8], B[4][8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const float a0 = A[0][k], a1 = A[1][k], a2 = A[2][k], a3 = A[3][k];
-            const float b0 = B[0][k], b1 = B[1][k], b2 = B[2][k], b3 = B[3][k];
-            /* CLT-domain correlation of the two tiles */
-            const float r0 = __fmaf_rn(a3, b3, __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, a0 * b0)));
-            const float r1 = __fmaf_rn(a2, b3, __fmaf_rn(-a3, b2, __fmaf_rn(a0, b1, -a1 * b0)));
-            const float r2 = __fmaf_rn(a1, b3, __fmaf_rn(a0, b2, __fmaf_rn(-a3, b1, -a2 * b0)));
-            const float r3 = __fmaf_rn(a0, b3, __fmaf_rn(-a1, b2, __fmaf_rn(-a2, b1, a3 * b0)));
-            acc[0][k] = __fmaf_rn(s, r0, acc[0][k]);
-            acc[1][k] = __fmaf_rn(s, r1, acc[1][k]);
-            acc[2][k] = __fmaf_rn(s, r2, acc[2][k]);
-            acc[3][k] = __fmaf_rn(s, r3, acc[3][k]);
+            for (int q = 0; q < 4; q++) {
+                const float *pa = a + color * cstride + q * 64 + l * 8 + k0;
+                const float *pb = b + color * cstride + q * 64 + l * 8 + k0;
+                if (KC == 8) {
+                    load_row8(pa, al16, A[q]);
+                    load_row8(pb, al16, B[q]);
+                } else {
+                    load_row4(pa, al16, A[q]);
+                    load_row4(pb, al16, B[q]);
+                }
+            }
+#pragma unroll
+            for (int kk = 0; kk < KC; kk++) {
+                const int k = k0 + kk;
+                const float a0 = A[0][kk], a1 = A[1][kk], a2 = A[2][kk], a3 = A[3][kk];
+                const float b0 = B[0][kk], b1 = B[1][kk], b2 = B[2][kk], b3 = B[3][kk];
+                /* CLT-domain correlation of the two tiles */
+                const float r0 = __fmaf_rn(a3, b3, __fmaf_rn(a2, b2, __fmaf_rn(a1, b1, a0 * b0)));
+                const float r1 = __fmaf_rn(a2, b3, __fmaf_rn(-a3, b2, __fmaf_rn(a0, b1, -a1 * b0)));
+                const float r2 = __fmaf_rn(a1, b3, __fmaf_rn(a0, b2, __fmaf_rn(-a3, b1, -a2 * b0)));
+                const float r3 = __fmaf_rn(a0, b3, __fmaf_rn(-a1, b2, __fmaf_rn(-a2, b1, a3 * b0)));
+                acc[0][k] = __fmaf_rn(s, r0, acc[0][k]);
+                acc[1][k] = __fmaf_rn(s, r1, acc[1][k]);
+                acc[2][k] = __fmaf_rn(s, r2, acc[2][k]);
+                acc[3][k] = __fmaf_rn(s, r3, acc[3][k]);
+            }
         }
         if (color == 1) { /* LPF after red and blue */
             float f[8];

@@ -187,12 +187,16 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
  * sd: debayered tiles D; sm: the plain (not debayered) tiles, scaled by
  * m_scale (the plain tile is the un-windowed one times the squared window);
  * both [job = cam * colors + color] with the given strides, pixel offset e.
- * o: colours, alpha, 4 port weights and (keep_weights) colors + 1 rms. */
+ * chw: the colour weights; chws: their square roots.
+ * o: colours, alpha, 4 port weights and (keep_weights) colors + 1 rms.
+ * The colour distances sum_col chw[col] ((X[col] - Y[col]) wi)^2 are formed
+ * as sum_col (X'[col] - Y'[col])^2 in the scaled space X' = X wi sqrt(chw),
+ * the same quantity with fewer operations per camera pair. */
 template <int COLORS>
 __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, const float *sm, int sm_stride,
                                               float m_scale, int e, const float *pd2r, float ksigma,
-                                              const float *chw, float wnd2, float wi, int dust_remove,
-                                              int keep_weights, float *o)
+                                              const float *chw, const float *chws, float wnd2, float wi,
+                                              int dust_remove, int keep_weights, float *o)
 {
     float D[4][COLORS];
 #pragma unroll
@@ -218,6 +222,13 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
         }
         o[COLORS + 5 + COLORS] = sqrtf(sw);
     }
+    /* D in the scaled space */
+#pragma unroll
+    for (int col = 0; col < COLORS; col++) {
+        const float sc = wi * chws[col];
+#pragma unroll
+        for (int cam = 0; cam < 4; cam++) D[cam][col] *= sc;
+    }
     /* wi = 1 / wnd2 correctly rounded (the reference forms it in double).
      * A weight is exp(...) plus the 1e-4 floor added in double and rounded
      * once to float, as the reference's double floor constant makes it: the
@@ -238,8 +249,8 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
                 float d = 0.0f;
 #pragma unroll
                 for (int col = 0; col < COLORS; col++) {
-                    const float dc = (D[i][col] - D[j][col]) * wi;
-                    d = __fmaf_rn(chw[col] * dc, dc, d);
+                    const float dc = D[i][col] - D[j][col];
+                    d = __fmaf_rn(dc, dc, d);
                 }
                 const float x = __double2float_rn((double)__expf(-pd2r[k] * d) + 1e-4);
                 pw[i] += x;
@@ -247,18 +258,19 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
                 k++;
             }
     }
+    /* the best two cameras (first of equals), their weights carried beside
+     * the indices: an array indexed by a run-time camera would live in local
+     * memory */
     int b1 = 0;
+    float p1 = pw[0];
 #pragma unroll
-    for (int cam = 1; cam < 4; cam++) if (pw[cam] > pw[b1]) b1 = cam;
+    for (int cam = 1; cam < 4; cam++)
+        if (pw[cam] > p1) { b1 = cam; p1 = pw[cam]; }
     int b2 = (b1 == 0) ? 1 : 0;
+    float p2 = (b1 == 0) ? pw[1] : pw[0];
 #pragma unroll
-    for (int cam = 1; cam < 4; cam++) if (cam > b2 && cam != b1 && pw[cam] > pw[b2]) b2 = cam;
-    float p1 = 0.0f, p2 = 0.0f;
-#pragma unroll
-    for (int cam = 0; cam < 4; cam++) {
-        if (cam == b1) p1 = pw[cam];
-        if (cam == b2) p2 = pw[cam];
-    }
+    for (int cam = 1; cam < 4; cam++)
+        if (cam > b2 && cam != b1 && pw[cam] > p2) { b2 = cam; p2 = pw[cam]; }
     const float w1 = __fdividef(p1, p1 + p2);
     const float w2 = 1.0f - w1;
     float avg[COLORS];
@@ -277,18 +289,17 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
         float d2 = 0.0f;
 #pragma unroll
         for (int col = 0; col < COLORS; col++) {
-            const float dc = (D[cam][col] - avg[col]) * wi;
-            d2 = __fmaf_rn(chw[col] * dc, dc, d2);
+            const float dc = D[cam][col] - avg[col];
+            d2 = __fmaf_rn(dc, dc, d2);
         }
         pw[cam] = __double2float_rn((double)__expf(-ksigma * d2) + 1e-4);
     }
     if (dust_remove) {
         int worst = 0;
+        float wv = pw[0];
 #pragma unroll
-        for (int cam = 1; cam < 4; cam++) if (pw[cam] < pw[worst]) worst = cam;
-        float wv = 0.0f;
-#pragma unroll
-        for (int cam = 0; cam < 4; cam++) if (cam == worst) wv = pw[cam];
+        for (int cam = 1; cam < 4; cam++)
+            if (pw[cam] < wv) { worst = cam; wv = pw[cam]; }
         float a = -wv;
 #pragma unroll
         for (int cam = 0; cam < 4; cam++) a += pw[cam];
@@ -303,11 +314,14 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
 #pragma unroll
     for (int cam = 0; cam < 4; cam++) ksum += pw[cam];
     const float kinv = __frcp_rn(ksum);
+    float kw[4];
+#pragma unroll
+    for (int cam = 0; cam < 4; cam++) kw[cam] = kinv * pw[cam];
 #pragma unroll
     for (int col = 0; col < COLORS; col++) {
         float v = 0.0f;
 #pragma unroll
-        for (int cam = 0; cam < 4; cam++) v = __fmaf_rn(kinv * pw[cam], sm[(cam * COLORS + col) * sm_stride + e], v);
+        for (int cam = 0; cam < 4; cam++) v = __fmaf_rn(kw[cam], sm[(cam * COLORS + col) * sm_stride + e], v);
         o[col] = v * m_scale;
     }
     o[COLORS] = wnd2 * ksum / 4.0f;
@@ -326,7 +340,7 @@ constexpr size_t kTexSmemBytes = sizeof(float) * kTexSmemFloats;
  * k_tc_stage<InvTcStage> writes them (the un-windowed T for colour, the
  * windowed M for mono, [16][16] row-major at the job's CLT offset): stage 1
  * copies the tile into shared memory instead of inverting the CLT. */
-template <bool FROM_T>
+template <bool FROM_T, bool ALL>
 __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     Geom g, const int *__restrict__ woi, float *const *clt, long long num_texture_tiles,
     const int *__restrict__ list, const int *__restrict__ dev_counts, int count_slot, int list_cap,
@@ -338,7 +352,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     float *s_t = smem;                 /* un-windowed tiles T (colour) or windowed M (mono) */
     float *s_x = s_t + 12 * kJob;      /* transposes, then the debayered tiles D            */
     __shared__ float *s_cp[4];
-    __shared__ float s_pd2r[6], s_chw[3];
+    __shared__ float s_pd2r[6], s_chw[3], s_chws[3];
 
     const int tid = threadIdx.x;
     const int l = tid & 7, grp = tid >> 3;
@@ -356,6 +370,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
                 s_pd2r[k++] = ksigma / (dx * dx + dy * dy);
             }
         s_chw[0] = p.w0; s_chw[1] = p.w1; s_chw[2] = p.w2;
+        for (int c = 0; c < 3; c++) s_chws[c] = sqrtf(s_chw[c]);
     }
 
     long long count = num_texture_tiles;
@@ -384,7 +399,8 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     /* list entry n of this pass */
     auto code_at = [&](long long n) -> int { return lst[n + (n >= split ? gap : 0)]; };
     const bool want_rbg = texture_rbg && texture_rbg_stride;
-    const bool want_tiles = texture_tiles && texture_stride;
+    const bool want_tiles = ALL && texture_tiles && texture_stride;
+    const int keep_weights = ALL ? p.keep_weights : 0;
     const int ns_tiles = (colors == 3) ? (p.keep_weights ? 12 : 4) : (p.keep_weights ? 8 : 2);
     int wx0 = 0, wy0 = 0, wh = 0;
     if (want_rbg) { wx0 = woi[0]; wy0 = woi[1]; wh = woi[3]; }
@@ -516,11 +532,11 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
             const float wnd2 = __ldg(&d_tex_wnd2[px]), wi = __ldg(&d_tex_wi[px]);
             float o[12];
             if (colors == 3)
-                combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, wnd2, wi, p.dust_remove,
-                                 p.keep_weights, o);
+                combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
+                                 p.dust_remove, keep_weights, o);
             else
-                combine_pixel<1>(s_t, kJob, s_t, kJob, 1.0f, e, s_pd2r, ksigma, s_chw, wnd2, wi, p.dust_remove,
-                                 p.keep_weights, o);
+                combine_pixel<1>(s_t, kJob, s_t, kJob, 1.0f, e, s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
+                                 p.dust_remove, keep_weights, o);
             if (want_tiles) {
                 float *dst = texture_tiles + (size_t)n * texture_stride + px;
 #pragma unroll
