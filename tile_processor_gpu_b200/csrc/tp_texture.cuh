@@ -42,90 +42,84 @@ constexpr int kJob = 280;        /* floats per 16x17 job tile, padded */
 
 __device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
 
-/* Per-pixel factors of the unfold, [16][17] (row stride 17: the eight lanes
- * of a group read eight rows of one column from distinct banks):
+/* Per-pixel factors of the unfold, [16][17]:
  *   tfac[r][c] = (0.25 / w[c]) / w[r]     un-windowed tile T = d * tfac
  *   mfac[r][c] = (0.5 w[r]) (0.5 w[c])    windowed tile M = mfac * d
- * with w the half-sine window, in the rounding order of the per-pixel form. */
+ * with w the half-sine window, as read-only tables in global memory for the
+ * tensor-core inverse stage's epilogue (values bit-identical to the float
+ * expressions, generated by gen_tables.py); and the squared window at each
+ * of the 256 pixels with its reciprocal for the camera fusion. */
 constexpr int kFac = 16 * 17;
-/* The same factors, and the squared window at each of the 256 pixels with its
- * reciprocal, as read-only tables in global memory for k_textures (values
- * bit-identical to the float expressions above and in the kernel's fusion,
- * generated by gen_tables.py); the lanes read them through the read-only
- * cache, which leaves the kernel's shared memory to its tiles. */
 __device__ float d_tex_tfac[kFac] = TP_TEX_TFAC_INIT;
 __device__ float d_tex_mfac[kFac] = TP_TEX_MFAC_INIT;
 __device__ float d_tex_wnd2[256] = TP_TEX_WND2_INIT;
 __device__ float d_tex_wi[256] = TP_TEX_WI_INIT;
-__device__ __forceinline__ void fill_unfold_factors(float *tfac, float *mfac, int tid, int nthreads)
-{
-    for (int i = tid; i < 256; i += nthreads) {
-        const int r = i >> 4, c = i & 15;
-        const float hr = c_hwin[r], hc = c_hwin[c];
-        tfac[r * 17 + c] = (0.25f / hc) / hr;
-        mfac[r * 17 + c] = (0.5f * hr) * (0.5f * hc);
-    }
-}
 
 /* Windowed inverse CLT of one job (imclt8threads, :3847-4017) into the
  * [16][17] tile M = w * d (w the product of the two half-sine windows, no
  * accumulation), and, for the debayer, the same tile with the squared window
  * removed, T = M / (sin^2 r sin^2 c) = d / (4 sin r sin c), formed directly
- * from the signed sum d.  Lane l ends the two passes holding pixel-domain row
- * l of all four quadrants in registers; the unfold (fold row RIND[r] = l for
- * exactly two output rows r) then writes those two rows whole, the quadrant
- * signs of idct_signs (:399-420) factored into a vertical sign per row and a
- * horizontal sign per column.  src: the job's 4x64 coefficients (row stride
- * 8) in shared memory; tb: the group's transpose buffer.  Either of mout and
- * tout may be NULL (with its factor table). */
+ * from the signed sum d.  Per quadrant, lane l loads coefficient row l (two
+ * 16-byte loads where the source allows), applies the low-pass filter, runs
+ * the horizontal DCT-IV/DST-IV on it, and after a transpose the vertical one
+ * on column l: it ends holding pixel-domain column l of all four quadrants.
+ * The unfold (fold column RIND[c] = l for exactly two output columns c) then
+ * writes those two columns whole, the quadrant signs of idct_signs
+ * (:399-420) factored into a horizontal sign pair per column (per lane) and
+ * a vertical sign per row (compile-time); the window factors are a per-lane
+ * column factor times a compile-time row factor.  The first column a lane
+ * writes is 11 - l: with job buffers 280 floats apart the four groups of a
+ * warp then store to 32 distinct banks in both columns.  src: the job's
+ * 4x64 coefficients (row stride 8), shared or global memory; tb: the
+ * group's transpose buffer.  Either of mout and tout may be NULL. */
 __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *mout,
-                                                 float *tout, const float *tfac, const float *mfac, int l,
-                                                 unsigned gm, int hswap = 0)
+                                                 float *tout, int l, unsigned gm)
 {
-    float a[4][8]; /* pixel-domain row l of each quadrant */
-    float f[8];    /* column l of the low-pass filter, shared by the quadrants */
-#pragma unroll
-    for (int m = 0; m < 8; m++) f[m] = lpf ? __ldg(&lpf[m * 8 + l]) : 1.0f;
+    constexpr float kHwin[16] = TP_HWIN_INIT;
+    float a[4][8]; /* pixel-domain column l of each quadrant */
+    float f[8];    /* row l of the low-pass filter, shared by the quadrants */
+    if (lpf)
+        load_row8(lpf + l * 8, true, f);
+    const bool al16 = !(reinterpret_cast<uintptr_t>(src) & 15);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        float col[8], v[8], row[8];
+        float row[8], v[8], col[8];
+        load_row8(src + q * 64 + l * 8, al16, row);
+        if (lpf) {
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
-            const float x = src[q * 64 + m * 8 + l];
-            col[m] = lpf ? x * f[m] : x;
+            for (int k = 0; k < 8; k++) row[k] *= f[k];
         }
-        if (q >> 1) dtt8<1>(col, v); else dtt8<0>(col, v);
+        if (q & 1) dtt8<1>(row, v); else dtt8<0>(row, v);
 #pragma unroll
-        for (int k = 0; k < 8; k++) tb[TBI(q, k, l)] = v[k];
+        for (int k = 0; k < 8; k++) tb[TBI(q, l, k)] = v[k];
         __syncwarp(gm);
 #pragma unroll
-        for (int k = 0; k < 8; k++) row[k] = tb[TBI(q, l, k)];
-        if (q & 1) dtt8<1>(row, a[q]); else dtt8<0>(row, a[q]);
+        for (int k = 0; k < 8; k++) col[k] = tb[TBI(q, k, l)];
+        if (q >> 1) dtt8<1>(col, a[q]); else dtt8<0>(col, a[q]);
     }
-    /* the two output rows folding onto row l, and their vertical signs
-     * (rows 0-3: +,+; 4-7: -,+; 8-11: -,+; 12-15: -,-) */
-    /* hswap (odd groups of a warp in k_textures) writes the two rows in the
-     * other order: with job buffers 280 floats apart, the four groups' rows
-     * of one store then fall in disjoint banks */
-#pragma unroll 1
-    for (int hh = 0; hh < 2; hh++) {
-        const int h = hh ^ hswap;
-        const int r = (l >= 4) ? (h ? 11 - l : l - 4) : (h ? l + 12 : 11 - l);
-        const int rq = r >> 2;
-        const bool n01 = rq != 0, n23 = rq == 3;
 #pragma unroll
-        for (int c = 0; c < 16; c++) {
-            const int v = (c < 4) ? c + 4 : (c < 12) ? 11 - c : c - 12;
-            const int cq = c >> 2;
-            /* (shc a0 + shs a1), (shc a2 + shs a3): shc = + for columns 0-3,
-             * shs = - for columns 12-15 */
-            const float e0 = (cq == 0) ? ((cq == 3) ? a[0][v] - a[1][v] : a[0][v] + a[1][v])
-                                       : ((cq == 3) ? -a[0][v] - a[1][v] : a[1][v] - a[0][v]);
-            const float e1 = (cq == 0) ? ((cq == 3) ? a[2][v] - a[3][v] : a[2][v] + a[3][v])
-                                       : ((cq == 3) ? -a[2][v] - a[3][v] : a[3][v] - a[2][v]);
-            const float d = (n01 ? -e0 : e0) + (n23 ? -e1 : e1);
-            if (mout) mout[JT(r, c)] = mfac[r * 17 + c] * d;
-            if (tout) tout[JT(r, c)] = d * tfac[r * 17 + c];
+    for (int h = 0; h < 2; h++) {
+        /* the output column and its quarter (columns 0-3: (+,+); 4-11:
+         * (-,+); 12-15: (-,-) on the (even, odd) quadrant of each pair) */
+        const int c = h ? ((l < 4) ? l + 12 : l - 4) : 11 - l;
+        const int cq = c >> 2;
+        const float s0 = (cq == 0) ? 1.0f : -1.0f, s1 = (cq == 3) ? -1.0f : 1.0f;
+        const float wc = __ldg(&d_hwin[c]);
+        const float tcol = 0.25f / wc, mcol = 0.5f * wc;
+        float e0[8], e1[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            e0[u] = __fmaf_rn(s0, a[0][u], s1 * a[1][u]);
+            e1[u] = __fmaf_rn(s0, a[2][u], s1 * a[3][u]);
+        }
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            const int u = (r < 4) ? r + 4 : (r < 12) ? 11 - r : r - 12;
+            const int rq = r >> 2;
+            /* vertical signs: rows 0-3 (+,+); 4-11 (-,+); 12-15 (-,-) */
+            const float d = ((rq != 0) ? -e0[u] : e0[u]) + ((rq == 3) ? -e1[u] : e1[u]);
+            if (mout) mout[JT(r, c)] = (d * mcol) * (0.5f * kHwin[r]);
+            if (tout) tout[JT(r, c)] = (d * tcol) * (1.0f / kHwin[r]);
         }
     }
 }
@@ -133,21 +127,31 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
 /* 3x3 debayer of the un-windowed tile T (interior 14x14; border copied),
  * shot-noise square root, squared window re-applied: T -> D
  * (debayer_shot / debayer, :4019-4199).  Lane l: columns l and l + 8, each
- * walked down with a 3x3 register window. */
+ * walked down with a 3x3 register window.  The stencil's horizontal pair
+ * t[r][c-1] + t[r][c+1] is summed once per row and shared by the three rows
+ * that use it; red/blue (rb_mode) and green take one branch-free form (the
+ * diagonal term's weight is 0 for green), so the groups of a warp, which
+ * hold different colours, do not diverge; the shot-noise scale and the two
+ * window factors are one product per pixel. */
 __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mode, float min_shot,
                                             float scale_shot, int l, unsigned gm)
 {
+    /* the window as compile-time constants (the values of c_hwin): the
+     * squared window of an unrolled row folds into an immediate operand */
+    constexpr float kHwin[16] = TP_HWIN_INIT;
     __syncwarp(gm);
     const float kshot = rsqrtf(min_shot);
+    const bool shot = scale_shot > 0.0f;
+    const float kdiag = rb_mode ? 0.0625f : 0.0f, kcenter = rb_mode ? 0.25f : 0.5f;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const int c = l + 8 * h;
         const bool cborder = (c == 0) || (c == 15);
         const int cm = cborder ? c : c - 1, cp = cborder ? c : c + 1;
         const float hcc = __ldg(&d_hwin[c]);
-        const float wx = hcc * hcc;
-        float a0 = t[JT(0, cm)], a1 = t[JT(0, c)], a2 = t[JT(0, cp)];
-        float b0 = t[JT(1, cm)], b1 = t[JT(1, c)], b2 = t[JT(1, cp)];
+        const float swx = (shot ? scale_shot : 1.0f) * (hcc * hcc);
+        float a1 = t[JT(0, c)], ha = t[JT(0, cm)] + t[JT(0, cp)];
+        float b1 = t[JT(1, c)], hb = t[JT(1, cm)] + t[JT(1, cp)];
 #pragma unroll
         for (int r = 0; r < 16; r++) {
             float v;
@@ -156,28 +160,22 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
             } else if (r == 15) {
                 v = b1;
             } else {
-                const float e0 = t[JT(r + 1, cm)], e1 = t[JT(r + 1, c)], e2 = t[JT(r + 1, cp)];
+                const float e1 = t[JT(r + 1, c)], he = t[JT(r + 1, cm)] + t[JT(r + 1, cp)];
                 if (cborder) {
                     v = b1;
                 } else {
-                    const float orth = ((a1 + e1) + b0) + b2;
-                    if (rb_mode) {
-                        const float diag = ((a0 + a2) + e0) + e2;
-                        v = __fmaf_rn(0.0625f, diag, __fmaf_rn(0.125f, orth, 0.25f * b1));
-                    } else {
-                        v = __fmaf_rn(0.125f, orth, 0.5f * b1);
-                    }
+                    const float orth = (a1 + e1) + hb;
+                    const float diag = ha + he;
+                    v = __fmaf_rn(kdiag, diag, __fmaf_rn(0.125f, orth, kcenter * b1));
                 }
-                a0 = b0; a1 = b1; a2 = b2;
-                b0 = e0; b1 = e1; b2 = e2;
+                a1 = b1; ha = hb;
+                b1 = e1; hb = he;
             }
             /* shot-noise square root above min_shot: v / sqrt(v) from the
              * hardware reciprocal square root (within 3e-7 of sqrtf), cheap
              * enough to evaluate on both sides of the select */
-            if (scale_shot > 0.0f)
-                v = scale_shot * ((v > min_shot) ? v * rsqrtf(fmaxf(v, 1e-30f)) : (kshot * v));
-            const float hr = c_hwin[r];
-            d[JT(r, c)] = v * (wx * (hr * hr));
+            if (shot) v = (v > min_shot) ? v * rsqrtf(fmaxf(v, 1e-30f)) : (kshot * v);
+            d[JT(r, c)] = v * (swx * (kHwin[r] * kHwin[r]));
         }
     }
     __syncwarp(gm);
@@ -506,12 +504,11 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
             if (colors > 1) {
                 /* T -> s_t, then the debayered D -> s_x (the transpose
                  * buffer, free once the unfold has read it) */
-                imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[color], xj, nullptr, tj,
-                                 d_tex_tfac, nullptr, l, gm, grp & 1);
+                imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[color], xj, nullptr, tj, l,
+                                 gm);
                 debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
             } else {
-                imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[3], xj, tj, nullptr,
-                                 nullptr, d_tex_mfac, l, gm, grp & 1);
+                imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[3], xj, tj, nullptr, l, gm);
             }
         }
         __syncthreads();
