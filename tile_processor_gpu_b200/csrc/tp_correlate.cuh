@@ -19,9 +19,8 @@
 
 namespace tp {
 
-/* per-group buffer: four 8x9 quadrants (transpose, then the pixel-domain
- * quadrants), then the (2r+1)^2 output staging; 536 % 32 == 24 */
-constexpr int kCorrBuf = 4 * 72 + 8 + 240;
+/* per-group buffer: four 8x9 quadrant transposes; 296 % 32 == 8 */
+constexpr int kCorrBuf = 4 * 72 + 8;
 
 /* 4 consecutive floats at p (16-byte aligned when al16) */
 __device__ __forceinline__ void load_row4(const float *p, bool al16, float v[4])
@@ -60,7 +59,6 @@ __device__ __forceinline__ void corr_job(const float *a, const float *b, int cst
                                          float *__restrict__ dst, int l, unsigned gm)
 {
     const int sz = 2 * r + 1;
-    float *stage = tb + 296;
     const bool al16 = !((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) |
                          (uintptr_t)(cstride * sizeof(float))) & 15);
     float acc[4][8]; /* row l of each quadrant */
@@ -127,7 +125,8 @@ __device__ __forceinline__ void corr_job(const float *a, const float *b, int cst
     }
     /* pixel domain: horizontal DCT-II (q0,q2) / DST-II (q1,q3) on the held
      * row, transpose, vertical DCT-II (q0,q1) / DST-II (q2,q3) on the held
-     * column, which replaces that column of its transpose buffer */
+     * column: lane l ends holding column l of each quadrant, p[q][i] = row i */
+    float p[4][8];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         float v[8], col[8];
@@ -137,28 +136,36 @@ __device__ __forceinline__ void corr_job(const float *a, const float *b, int cst
         __syncwarp(gm);
 #pragma unroll
         for (int k = 0; k < 8; k++) col[k] = tb[TBI(q, k, l)];
-        if (q >> 1) dtt8<3>(col, v); else dtt8<2>(col, v);
-#pragma unroll
-        for (int k = 0; k < 8; k++) tb[TBI(q, k, l)] = v[k];
+        if (q >> 1) dtt8<3>(col, p[q]); else dtt8<2>(col, p[q]);
     }
-    __syncwarp(gm);
-    /* unfold (lane i = rows +-i): R[+-i][+-j] from q0[i][j], q1[i][j-1],
-     * q2[i-1][j], q3[i-1][j-1], scaled by 1/4 */
+    __syncwarp(gm); /* the transpose buffer free for the group's next job */
+    /* unfold, lane j = columns r +- j: R[+-i][+-j] from q0[i][j], q1[i][j-1]
+     * (lane j - 1), q2[i-1][j], q3[i-1][j-1], scaled by 1/4, stored straight
+     * to dst (each store of a group covers 8 consecutive floats of a row) */
+    float q1l[8], q3l[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        q1l[i] = __shfl_up_sync(gm, p[1][i], 1, 8);
+        q3l[i] = __shfl_up_sync(gm, p[3][i], 1, 8);
+    }
     if (l <= r) {
-        for (int j = 0; j <= r; j++) {
-            const float q0 = tb[TBI(0, l, j)];
-            const float q1 = j > 0 ? tb[TBI(1, l, j - 1)] : 0.0f;
-            const float q2 = l > 0 ? tb[TBI(2, l - 1, j)] : 0.0f;
-            const float q3 = (l > 0 && j > 0) ? tb[TBI(3, l - 1, j - 1)] : 0.0f;
-            stage[(r + l) * sz + (r + j)] = 0.25f * ((q0 + q1) + (q2 + q3));
-            stage[(r + l) * sz + (r - j)] = 0.25f * ((q0 - q1) + (q2 - q3));
-            stage[(r - l) * sz + (r + j)] = 0.25f * ((q0 + q1) - (q2 + q3));
-            stage[(r - l) * sz + (r - j)] = 0.25f * ((q0 - q1) - (q2 - q3));
+        const int j = l;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            if (i > r) break;
+            const float q0 = p[0][i];
+            const float q1 = j > 0 ? q1l[i] : 0.0f;
+            const float q2 = i > 0 ? p[2][i - 1] : 0.0f;
+            const float q3 = (i > 0 && j > 0) ? q3l[i - 1] : 0.0f;
+            /* in this order: where i or j is 0 the later store to the same
+             * element is the one that stays */
+            float *up = dst + (r + i) * sz + r, *dn = dst + (r - i) * sz + r;
+            up[j] = 0.25f * ((q0 + q1) + (q2 + q3));
+            up[-j] = 0.25f * ((q0 - q1) + (q2 - q3));
+            dn[j] = 0.25f * ((q0 + q1) - (q2 + q3));
+            dn[-j] = 0.25f * ((q0 - q1) - (q2 - q3));
         }
     }
-    __syncwarp(gm);
-    for (int k = l; k < sz * sz; k += 8) dst[k] = stage[k];
-    __syncwarp(gm);
 }
 
 __global__ void __launch_bounds__(128, 4) k_correlate2D(Geom g, float *const *clt, int colors,
