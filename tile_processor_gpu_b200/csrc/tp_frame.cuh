@@ -222,18 +222,23 @@ __global__ void __launch_bounds__(kFrameThreads, kFrameBlocksPerSm) k_frame(
             for (int px = tid; px < 256; px += kFrameThreads) {
                 const int r = px >> 4, c = px & 15;
                 const float wnd2 = __ldg(&d_tex_wnd2[px]), wi = __ldg(&d_tex_wi[px]);
+                /* the pixel's RGBA values, loaded before the fusion covers their latency */
+                const int gy = gy0 + r, gx = gx0 + c;
+                float *b = (gy < 0 || gx < 0) ? nullptr : rgba + (size_t)gy * rgba_stride + (size_t)gx;
+                float old[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                if (b) {
+#pragma unroll
+                    for (int sl = 0; sl < 4; sl++) old[sl] = b[(size_t)sl * slice_stride];
+                }
                 float o[12];
                 combine_pixel<3>(s_x, kTB4, s_clt, kJob, wnd2, JT(r, c), s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
                                  p.tex.dust_remove, 0, o);
-                const int gy = gy0 + r, gx = gx0 + c;
-                if (gy < 0 || gx < 0) continue;
-                float *b = rgba + (size_t)gy * rgba_stride + (size_t)gx;
+                if (!b) continue;
                 const float f = (nbr != TP_TASK_TEXTURE_BITS) ? __ldg(&d_alpha_fade[nbr][px]) : 1.0f;
 #pragma unroll
                 for (int sl = 0; sl < 4; sl++) {
                     const float v = (nbr != TP_TASK_TEXTURE_BITS) ? o[sl] * f : o[sl];
-                    float *q = b + (size_t)sl * slice_stride;
-                    *q = *q + v;
+                    b[(size_t)sl * slice_stride] = old[sl] + v;
                 }
             }
         }

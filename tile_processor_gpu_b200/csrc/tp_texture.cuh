@@ -59,8 +59,9 @@ __device__ float d_tex_wi[256] = TP_TEX_WI_INIT;
  * [16][17] tile M = w * d (w the product of the two half-sine windows, no
  * accumulation), and, for the debayer, the same tile with the squared window
  * removed, T = M / (sin^2 r sin^2 c) = d / (4 sin r sin c), formed directly
- * from the signed sum d.  Per quadrant, lane l loads coefficient row l (two
- * 16-byte loads where the source allows), applies the low-pass filter, runs
+ * from the signed sum d.  Lane l loads coefficient row l of each quadrant (two
+ * 16-byte loads per row where the source allows); per quadrant it applies
+ * the low-pass filter, runs
  * the horizontal DCT-IV/DST-IV on it, and after a transpose the vertical one
  * on column l: it ends holding pixel-domain column l of all four quadrants.
  * The unfold (fold column RIND[c] = l for exactly two output columns c) then
@@ -81,10 +82,15 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
     if (lpf)
         load_row8(lpf + l * 8, true, f);
     const bool al16 = !(reinterpret_cast<uintptr_t>(src) & 15);
+    /* all four rows in flight before the first transform needs one */
+    float raw[4][8];
+#pragma unroll
+    for (int q = 0; q < 4; q++) load_row8(src + q * 64 + l * 8, al16, raw[q]);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         float row[8], v[8], col[8];
-        load_row8(src + q * 64 + l * 8, al16, row);
+#pragma unroll
+        for (int k = 0; k < 8; k++) row[k] = raw[q][k];
         if (lpf) {
 #pragma unroll
             for (int k = 0; k < 8; k++) row[k] *= f[k];
@@ -527,6 +533,15 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
             const int r = px >> 4, c = px & 15;
             const int e = JT(r, c);
             const float wnd2 = __ldg(&d_tex_wnd2[px]), wi = __ldg(&d_tex_wi[px]);
+            /* the pixel's RGBA values are loaded before the fusion, whose
+             * arithmetic then covers their latency */
+            float old[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            float *b = (want_rbg && nbr) ? rgba_at(gy0, gx0, px) : nullptr;
+            if (b) {
+#pragma unroll
+                for (int sl = 0; sl < 4; sl++)
+                    if (sl <= colors) old[sl] = b[(size_t)sl * slice_stride];
+            }
             float o[12];
             if (colors == 3)
                 combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
@@ -540,17 +555,13 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
                 for (int sl = 0; sl < 12; sl++)
                     if (sl < ns_tiles) dst[sl * 256] = o[sl];
             }
-            if (want_rbg && nbr) {
-                float *b = rgba_at(gy0, gx0, px);
-                if (b) {
-                    const float f = (nbr != TP_TASK_TEXTURE_BITS) ? __ldg(&d_alpha_fade[nbr][px]) : 1.0f;
+            if (b) {
+                const float f = (nbr != TP_TASK_TEXTURE_BITS) ? __ldg(&d_alpha_fade[nbr][px]) : 1.0f;
 #pragma unroll
-                    for (int sl = 0; sl < 4; sl++) {
-                        if (sl > colors) break;
-                        const float v = (nbr != TP_TASK_TEXTURE_BITS) ? o[sl] * f : o[sl];
-                        float *q = b + (size_t)sl * slice_stride;
-                        *q = *q + v;
-                    }
+                for (int sl = 0; sl < 4; sl++) {
+                    if (sl > colors) break;
+                    const float v = (nbr != TP_TASK_TEXTURE_BITS) ? o[sl] * f : o[sl];
+                    b[(size_t)sl * slice_stride] = old[sl] + v;
                 }
             }
         }
