@@ -71,15 +71,17 @@ def bench_config(world):
 
 
 def dram_traffic():
-    """DRAM bytes per frame of each stage from the ncu capture recorded with
-    the package (a capture, not a measurement of this run)"""
+    """DRAM bytes per frame of each stage (and of the fused frame kernel)
+    from the ncu captures recorded with the package (captures, not
+    measurements of this run): (per stage, source, fused bytes, fused source)"""
     path = os.path.join(ROOT, "tile_processor_gpu_b200", "data", "dram_traffic.json")
     try:
         with open(path) as fh:
             d = json.load(fh)
-        return d["bytes_per_frame"], "ncu capture: " + d["command"]
+        return (d["bytes_per_frame"], "ncu capture: " + d["command"], d.get("fused_frame_bytes"),
+                "ncu capture: " + d["fused_command"] if "fused_command" in d else None)
     except (OSError, ValueError, KeyError):
-        return {}, None
+        return {}, None, None, None
 
 
 def peaks():
@@ -812,7 +814,7 @@ def run_b200(args, rank, world, local, pg):
     achieved = algo[dom] / (stage_ms[dom] * 1e-3) / 1e9
     fps = world * frames_timed / (ms_max * 1e-3)
     flops = FLOPS_PER_TILE[dom] * pipe.num_tiles
-    traffic, traffic_source = dram_traffic()
+    traffic, traffic_source, fused_traffic, fused_source = dram_traffic()
     out = {
         "metric": METRIC, "value": round(fps, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
@@ -824,6 +826,10 @@ def run_b200(args, rank, world, local, pg):
         "path": "tp_convert_correct_tiles + tp_correlate2D + tp_generate_RBGA",
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "fused_frame_ms": round(fused_ms, 4),
+        "fused_frame": {"ms": round(fused_ms, 4), "dram_bytes": fused_traffic, "dram_source": fused_source,
+                        "staged_dram_bytes": int(sum(traffic.values())) if traffic else None,
+                        "compulsory_bytes": int(pipe.frame_bytes()),
+                        "hbm_frac_of_measured": round(pipe.frame_bytes() / (fused_ms * 1e-3) / 1e9 / hbm, 4)},
         "precision": {"what": "the same three calls with each stage's 8x8 transforms as tcgen05 GEMMs "
                               "(tp_*_tc: split 16-bit operands, three MMAs per product, FP32 accumulation); "
                               "errors against the FP64 oracle in parity.precision",

@@ -192,11 +192,12 @@ class DisparityMLP:
 # --------------------------------------------------------------------------- #
 # training data from the library's own pipeline
 # --------------------------------------------------------------------------- #
-def make_samples(seed, width=1024, height=768, disparity=(0.0, 32.0), error=1.0, margin=5, device="cuda"):
+def make_samples(seed, width=1024, height=768, disparity=(0.0, 32.0), error=1.0, margin=5, device="cuda", pool=64):
     """One synthetic plane-scene frame through convert, correlate and the plain
     fit.  Returns (features [n][1350], plain residual [n], true residual [n])
     as device tensors for the interior tiles (`margin` tiles from the edges,
-    where every camera's footprint stays inside the frame)."""
+    where every camera's footprint stays inside the frame).  pool: PSF
+    shapes of the frame's kernel tables."""
     torch = _t()
     from . import api, synth
     rng = np.random.default_rng(seed)
@@ -206,7 +207,7 @@ def make_samples(seed, width=1024, height=768, disparity=(0.0, 32.0), error=1.0,
     dstride = width + 64
     pitched = np.zeros((4, height + 16, dstride), np.float32)
     pitched[:, :height, :width] = imgs
-    kern, extra = synth.kernel_tables(rng, geom, pool=64, zero_extra=True, psf_offset=0.0)
+    kern, extra = synth.kernel_tables(rng, geom, pool=pool, zero_extra=True, psf_offset=0.0)
     tasks_np, err = synth.tasks_grid(geom, rng, jitter=0.0, disparity=disp, disparity_error=error,
                                      return_error=True)
     TX, TY, _ = synth.tiles(geom)
@@ -264,7 +265,10 @@ def gated(rho, logvar, plain, gate):
     return torch.where(logvar < gate, rho, plain)
 
 
-def choose_gate(rho, logvar, plain, truth, quantiles=(0.5, 0.6, 0.7, 0.8, 0.85, 0.9, 0.95, 0.98, 0.99)):
+GATE_QUANTILES = (0.5, 0.6, 0.7, 0.8, 0.85, 0.9, 0.95, 0.97, 0.98, 0.99, 0.995, 0.998, 0.999)
+
+
+def choose_gate(rho, logvar, plain, truth, quantiles=GATE_QUANTILES):
     """Pick the log-variance gate on validation samples: among +inf and the
     given quantiles of logvar, the one with the fewest > 0.5 px errors whose
     RMS error stays within 0.5% of the best RMS error.  Returns (gate, table)."""
