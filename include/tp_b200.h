@@ -420,6 +420,14 @@ int tp_mlp_features(const tp_geometry *g, const float *corrs, size_t corr_stride
  * C = gelu(z) (exact, erf form). */
 int tp_mlp_gemm(int M, int N, int K, const float *A, int lda, int trans_a, const float *B, int ldb, int trans_b,
                 float beta, float *C, int ldc, const float *bias, float *z, int ldz, tp_stream_t stream);
+/* The same operation on the tensor cores: each FP32 operand split into two
+ * TF32 parts (hi = tf32(x), lo = tf32(x - hi)), each product as three tcgen05
+ * TF32 MMAs (hi hi + hi lo + lo hi) accumulated in FP32 (about 21 significant
+ * bits per operand), tiles of 128 x 64 of C.  err (device int, may be NULL) is
+ * set to 1 if a wait for the tensor cores ran out (C is then not written). */
+int tp_mlp_gemm_tc(int M, int N, int K, const float *A, int lda, int trans_a, const float *B, int ldb, int trans_b,
+                   float beta, float *C, int ldc, const float *bias, float *z, int ldz, int *err,
+                   tp_stream_t stream);
 /* dz = dh * gelu'(z), rows x cols, leading dimension ld */
 int tp_mlp_gelu_backward(int rows, int cols, int ld, const float *z, const float *dh, float *dz,
                          tp_stream_t stream);

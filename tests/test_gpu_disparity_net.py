@@ -13,9 +13,16 @@ def _dev(a):
 
 
 @pytest.mark.parametrize("M,N,K,ta,tb", [(70, 37, 51, 0, 0), (130, 256, 1350, 0, 0), (1350, 256, 97, 1, 0),
-                                          (64, 128, 256, 0, 1), (33, 2, 128, 1, 1)])
+                                          (64, 128, 256, 0, 1), (33, 2, 128, 1, 1), (4096, 256, 1350, 0, 0),
+                                          (1350, 256, 4096, 1, 0), (256, 128, 4096, 1, 0), (300, 0, 7, 0, 0),
+                                          (200, 40, 0, 0, 0)])
 @pytest.mark.parametrize("epi", ["plain", "bias_beta", "gelu"])
-def test_gemm(native, oracle, M, N, K, ta, tb, epi):
+@pytest.mark.parametrize("tc", [False, True], ids=["simt", "tensor_core"])
+def test_gemm(native, oracle, M, N, K, ta, tb, epi, tc):
+    """tp_mlp_gemm (FP32 SIMT) and tp_mlp_gemm_tc (split-TF32 tensor-core
+    MMAs) against FP64, within 1e-5 of the largest magnitude; the
+    tensor-core GEMM's error flag stays clear.  K = 0 gives the epilogue of a
+    zero product; N = 0 leaves C alone."""
     import torch
     from tile_processor_gpu_b200 import disparity_net as D
     rng = np.random.default_rng(M * 7 + N)
@@ -25,21 +32,27 @@ def test_gemm(native, oracle, M, N, K, ta, tb, epi):
     bias = rng.standard_normal(N).astype(np.float32)
     a, b, c = _dev(A), _dev(B), _dev(C0)
     z = torch.zeros_like(c) if epi == "gelu" else None
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
     D.gemm(a, b, c, M, N, K, ta=ta, tb=tb, beta=0.5 if epi == "bias_beta" else 0.0,
-           bias=_dev(bias) if epi != "plain" else None, z=z)
+           bias=_dev(bias) if epi != "plain" else None, z=z, tc=tc, err=err)
     torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    if N == 0:
+        return
     ref = (A.T if ta else A).astype(np.float64) @ (B.T if tb else B).astype(np.float64)
     if epi != "plain":
         ref = ref + bias
     if epi == "bias_beta":
         ref = ref + 0.5 * C0
+    den = lambda r: np.abs(r).max() or 1.0  # noqa: E731  (K = 0 without bias: an all-zero product)
     if epi == "gelu":
-        assert np.max(np.abs(z.cpu().numpy() - ref)) / np.abs(ref).max() < 1e-5
+        assert np.max(np.abs(z.cpu().numpy() - ref)) / den(ref) < 1e-5
         ref = oracle.mlp_gelu(ref)
-    assert np.max(np.abs(c.cpu().numpy() - ref)) / np.abs(ref).max() < 1e-5
+    assert np.max(np.abs(c.cpu().numpy() - ref)) / den(ref) < 1e-5
 
 
-def test_gradients_against_oracle(native, oracle):
+@pytest.mark.parametrize("tc", [False, True], ids=["simt", "tensor_core"])
+def test_gradients_against_oracle(native, oracle, tc):
     import torch
     from tile_processor_gpu_b200 import disparity_net as D
     rng = np.random.default_rng(5)
@@ -51,11 +64,12 @@ def test_gradients_against_oracle(native, oracle):
     x = rng.normal(0, 0.3, (rows, D.N_IN)).astype(np.float32)
     t = rng.normal(0, 0.5, rows).astype(np.float32)
     w = (rng.random(rows) > 0.2).astype(np.float32)
-    net = D.DisparityMLP(p)
+    net = D.DisparityMLP(p, tc=tc)
     xd = _dev(x)
     out = net.forward(xd, rows)
     loss = net.loss_backward(xd, rows, _dev(t), weight=_dev(w))
     torch.cuda.synchronize()
+    net.check()
     ref_out, _ = oracle.mlp_forward(p, x.astype(np.float64))
     ref_loss, ref_g = oracle.mlp_loss_and_grads(p, x.astype(np.float64), t.astype(np.float64), w)
     assert np.max(np.abs(out.cpu().numpy() - ref_out)) / np.abs(ref_out).max() < 1e-5

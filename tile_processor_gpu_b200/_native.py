@@ -70,6 +70,7 @@ SIGNATURES = {
     "tp_corr_indices_from_tasks": [_P, _I, _I, _P],
     "tp_mlp_features": [_G, _P, _S, _I, _S, _P, _P, _S, _P],
     "tp_mlp_gemm": [_I, _I, _I, _P, _I, _I, _P, _I, _I, _F, _P, _I, _P, _P, _I, _P],
+    "tp_mlp_gemm_tc": [_I, _I, _I, _P, _I, _I, _P, _I, _I, _F, _P, _I, _P, _P, _I, _P, _P],
     "tp_mlp_gelu_backward": [_I, _I, _I, _P, _P, _P, _P],
     "tp_mlp_colsum": [_I, _I, _I, _P, _F, _P, _P],
     "tp_mlp_nll": [_I, _P, _P, _P, _F, _P, _P, _P],

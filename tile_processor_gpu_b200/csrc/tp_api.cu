@@ -31,6 +31,7 @@
 #include "tp_inv_tc.cuh"
 #include "tp_fwd_tc.cuh"
 #include "tp_mlp.cuh"
+#include "tp_gemm_tc.cuh"
 
 #define TP_VERSION "tile_processor_gpu_b200 0.1 (sm_100a)"
 
@@ -117,7 +118,7 @@ int shape_per_sm(int which)
  * their attribute once per device (the first call; make it before capturing
  * a stream into a graph). */
 std::mutex g_attr_mutex;
-bool g_tex_attr[4][128], g_frame_attr[128], g_tc_attr[128];
+bool g_tex_attr[4][128], g_frame_attr[128], g_tc_attr[128], g_gemm_tc_attr[128];
 
 int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
 {
@@ -739,7 +740,7 @@ int tp_mlp_gemm(int M, int N, int K, const float *A, int lda, int trans_a, const
 {
     if (M < 0 || N < 0 || K < 0) return fail(TP_ERR_ARG, "gemm %d x %d x %d", M, N, K);
     if (M == 0 || N == 0) return TP_OK;
-    if (!A || !B || !C) return fail(TP_ERR_ARG, "NULL gemm operand");
+    if (!C || (K > 0 && (!A || !B))) return fail(TP_ERR_ARG, "NULL gemm operand");
     if (lda < (trans_a ? M : K) || ldb < (trans_b ? K : N) || ldc < N || (z && ldz < N))
         return fail(TP_ERR_ARG, "gemm leading dimension too small");
     if ((M + tp::kGB - 1) / tp::kGB > 65535) return fail(TP_ERR_ARG, "gemm M %d too large", M);
@@ -747,6 +748,43 @@ int tp_mlp_gemm(int M, int N, int K, const float *A, int lda, int trans_a, const
     tp::k_gemm<<<grid, 256, 0, (cudaStream_t)stream>>>(M, N, K, A, lda, trans_a, B, ldb, trans_b, beta, C, ldc, bias,
                                                        z, ldz);
     return cuda_status(cudaGetLastError(), "mlp_gemm launch");
+}
+
+int tp_mlp_gemm_tc(int M, int N, int K, const float *A, int lda, int trans_a, const float *B, int ldb, int trans_b,
+                   float beta, float *C, int ldc, const float *bias, float *z, int ldz, int *err, tp_stream_t stream)
+{
+    if (M < 0 || N < 0 || K < 0) return fail(TP_ERR_ARG, "gemm %d x %d x %d", M, N, K);
+    if (M == 0 || N == 0) return TP_OK;
+    if (!C || (K > 0 && (!A || !B))) return fail(TP_ERR_ARG, "NULL gemm operand");
+    if (lda < (trans_a ? M : K) || ldb < (trans_b ? K : N) || ldc < N || (z && ldz < N))
+        return fail(TP_ERR_ARG, "gemm leading dimension too small");
+    if ((M + tp::kGtM - 1) / tp::kGtM > 65535) return fail(TP_ERR_ARG, "gemm M %d too large", M);
+    int rc;
+    if ((rc = set_smem_once(g_gemm_tc_attr, (const void *)tp::k_gemm_tc, tp::kGtSmemBytes,
+                            "cudaFuncSetAttribute(k_gemm_tc)")))
+        return rc;
+    int sms;
+    if ((rc = sm_count(&sms))) return rc;
+    dim3 grid((unsigned)((N + tp::kGtN - 1) / tp::kGtN), (unsigned)((M + tp::kGtM - 1) / tp::kGtM), 1);
+    /* A plain product (no bias, beta 0, no GELU) with fewer tiles than SMs and
+     * a long K (the weight gradients: K = the batch) splits K over up to
+     * 2 x SMs CTAs, each adding its partial sums into C, zeroed first (the
+     * order of those few additions per element is not fixed). */
+    const long long tiles = (long long)grid.x * grid.y;
+    const int chunks = (K + tp::kGtK - 1) / tp::kGtK;
+    if (!bias && !z && beta == 0.0f && tiles < sms && chunks >= 8) {
+        long long splits = (2LL * sms + tiles - 1) / tiles;
+        if (splits > chunks / 4) splits = chunks / 4;
+        if (splits > 1) {
+            grid.z = (unsigned)splits;
+            const cudaError_t e = cudaMemset2DAsync(C, (size_t)ldc * sizeof(float), 0, (size_t)N * sizeof(float),
+                                                    (size_t)M, (cudaStream_t)stream);
+            if (e != cudaSuccess) return cuda_status(e, "mlp_gemm_tc clear");
+        }
+    }
+    tp::k_gemm_tc<<<grid, 128, tp::kGtSmemBytes, (cudaStream_t)stream>>>(M, N, K, A, lda, trans_a, B, ldb, trans_b,
+                                                                       beta, C, ldc, bias, z, ldz, err);
+    return cuda_status(cudaGetLastError(), "mlp_gemm_tc launch");
 }
 
 int tp_mlp_gelu_backward(int rows, int cols, int ld, const float *z, const float *dh, float *dz, tp_stream_t stream)

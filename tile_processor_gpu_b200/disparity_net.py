@@ -49,14 +49,20 @@ def init_params(seed=0):
 
 
 def gemm(A, B, C, M, N, K, ta=0, tb=0, beta=0.0, bias=None, z=None, lda=None, ldb=None, ldc=None, ldz=None,
-         stream=None):
+         stream=None, tc=False, err=None):
+    """C = beta C + op(A) op(B) (+ bias; with z, z = that and C = gelu(z)):
+    tp_mlp_gemm_tc (split-TF32 tensor-core MMAs; err: device int32 set to 1
+    if a wait ran out) when tc, else tp_mlp_gemm (FP32 SIMT)."""
     lda = lda if lda is not None else (M if ta else K)
     ldb = ldb if ldb is not None else (K if tb else N)
     ldc = ldc if ldc is not None else N
     ldz = ldz if ldz is not None else N
-    _native.call("tp_mlp_gemm", int(M), int(N), int(K), _dptr(A), int(lda), int(ta), _dptr(B), int(ldb), int(tb),
-                 float(beta), _dptr(C), int(ldc), _dptr(bias) if bias is not None else None,
-                 _dptr(z) if z is not None else None, int(ldz), _stream(stream))
+    args = [int(M), int(N), int(K), _dptr(A), int(lda), int(ta), _dptr(B), int(ldb), int(tb), float(beta), _dptr(C),
+            int(ldc), _dptr(bias) if bias is not None else None, _dptr(z) if z is not None else None, int(ldz)]
+    if tc:
+        _native.call("tp_mlp_gemm_tc", *args, _dptr(err) if err is not None else None, _stream(stream))
+    else:
+        _native.call("tp_mlp_gemm", *args, _stream(stream))
 
 
 def features(geom, corrs, corr_stride, corr_radius, num_corr, corr_indices, out, feature_stride=N_IN,
@@ -78,10 +84,14 @@ def pad_rows(x, ldx=TC_LDX):
 class DisparityMLP:
     """Weights, Adam state and the forward / backward passes on the GPU."""
 
-    def __init__(self, params=None, device="cuda", seed=0):
+    def __init__(self, params=None, device="cuda", seed=0, tc=True):
         torch = _t()
         host = params if params is not None else init_params(seed)
         self.p = {k: torch.from_numpy(np.ascontiguousarray(host[k], np.float32)).to(device) for k in PARAMS}
+        # the forward and backward GEMMs on the tensor cores (tp_mlp_gemm_tc)
+        # or as FP32 SIMT (tp_mlp_gemm); _err is the tensor-core GEMM's flag
+        self.tc = tc
+        self._err = torch.zeros(1, dtype=torch.int32, device=device) if device != "cpu" else None
         self.g = {k: torch.zeros_like(v) for k, v in self.p.items()}
         self.m = {k: torch.zeros_like(v) for k, v in self.p.items()}
         self.v = {k: torch.zeros_like(v) for k, v in self.p.items()}
@@ -103,9 +113,12 @@ class DisparityMLP:
         keeps the activations for backward."""
         w = self._work(rows)
         p = self.p
-        gemm(x, p["W1"], w["h1"], rows, N_H1, N_IN, bias=p["b1"], z=w["z1"], lda=ldx, stream=stream)
-        gemm(w["h1"], p["W2"], w["h2"], rows, N_H2, N_H1, bias=p["b2"], z=w["z2"], stream=stream)
-        gemm(w["h2"], p["W3"], w["out"], rows, N_OUT, N_H2, bias=p["b3"], stream=stream)
+        gemm(x, p["W1"], w["h1"], rows, N_H1, N_IN, bias=p["b1"], z=w["z1"], lda=ldx,
+             stream=stream, tc=self.tc, err=self._err)
+        gemm(w["h1"], p["W2"], w["h2"], rows, N_H2, N_H1, bias=p["b2"], z=w["z2"],
+             stream=stream, tc=self.tc, err=self._err)
+        gemm(w["h2"], p["W3"], w["out"], rows, N_OUT, N_H2, bias=p["b3"],
+             stream=stream, tc=self.tc, err=self._err)
         return w["out"][:rows]
 
     def loss_backward(self, x, rows, target, weight=None, ldx=N_IN, stream=None):
@@ -118,22 +131,34 @@ class DisparityMLP:
                      _dptr(weight) if weight is not None else None, 1.0 / max(count, 1.0), _dptr(w["dout"]),
                      _dptr(w["loss"]), _stream(stream))
         # layer 3
-        gemm(w["h2"], w["dout"], g["W3"], N_H2, N_OUT, rows, ta=1, lda=N_H2, stream=stream)
+        gemm(w["h2"], w["dout"], g["W3"], N_H2, N_OUT, rows, ta=1, lda=N_H2,
+             stream=stream, tc=self.tc, err=self._err)
         _native.call("tp_mlp_colsum", int(rows), N_OUT, N_OUT, _dptr(w["dout"]), 1.0, _dptr(g["b3"]),
                      _stream(stream))
-        gemm(w["dout"], p["W3"], w["dh2"], rows, N_H2, N_OUT, tb=1, ldb=N_OUT, stream=stream)
+        gemm(w["dout"], p["W3"], w["dh2"], rows, N_H2, N_OUT, tb=1, ldb=N_OUT,
+             stream=stream, tc=self.tc, err=self._err)
         _native.call("tp_mlp_gelu_backward", int(rows), N_H2, N_H2, _dptr(w["z2"]), _dptr(w["dh2"]), _dptr(w["dz2"]),
                      _stream(stream))
         # layer 2
-        gemm(w["h1"], w["dz2"], g["W2"], N_H1, N_H2, rows, ta=1, lda=N_H1, stream=stream)
+        gemm(w["h1"], w["dz2"], g["W2"], N_H1, N_H2, rows, ta=1, lda=N_H1,
+             stream=stream, tc=self.tc, err=self._err)
         _native.call("tp_mlp_colsum", int(rows), N_H2, N_H2, _dptr(w["dz2"]), 1.0, _dptr(g["b2"]), _stream(stream))
-        gemm(w["dz2"], p["W2"], w["dh1"], rows, N_H1, N_H2, tb=1, ldb=N_H2, stream=stream)
+        gemm(w["dz2"], p["W2"], w["dh1"], rows, N_H1, N_H2, tb=1, ldb=N_H2,
+             stream=stream, tc=self.tc, err=self._err)
         _native.call("tp_mlp_gelu_backward", int(rows), N_H1, N_H1, _dptr(w["z1"]), _dptr(w["dh1"]), _dptr(w["dz1"]),
                      _stream(stream))
         # layer 1
-        gemm(x, w["dz1"], g["W1"], N_IN, N_H1, rows, ta=1, lda=ldx, stream=stream)
+        gemm(x, w["dz1"], g["W1"], N_IN, N_H1, rows, ta=1, lda=ldx,
+             stream=stream, tc=self.tc, err=self._err)
         _native.call("tp_mlp_colsum", int(rows), N_H1, N_H1, _dptr(w["dz1"]), 1.0, _dptr(g["b1"]), _stream(stream))
         return float(w["loss"][:rows].sum().item()) / max(count, 1.0)
+
+    def check(self):
+        """Raise if a tensor-core GEMM of this network reported a wait that ran
+        out (its flag is cleared for the next step)."""
+        if self._err is not None and int(self._err.item()):
+            self._err.zero_()
+            raise RuntimeError("tp_mlp_gemm_tc: a wait for the tensor cores ran out")
 
     def adam_step(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
         self.step_count += 1
@@ -253,6 +278,7 @@ def train(net, feats, plain, truth, epochs=4, batch=4096, lr=1e-3, seed=0, log=N
             total += net.loss_backward(xb, batch, tb)
             net.adam_step(lr=lr)
             nb += 1
+        net.check()
         if log is not None:
             log(ep, total / max(nb, 1))
     return net
