@@ -164,6 +164,17 @@ int tp_convert_correct_tiles(const tp_geometry *g,
                              int num_tiles,
                              int lpf_mask,
                              tp_stream_t stream);
+/* The same operation with the Bayer windows staged in shared memory by the
+ * TMA unit (one producer warp computes each job's geometry and bulk-copies
+ * the 16 x 20 window at the 16-byte boundary left of its corner; consumer
+ * warps fold from shared memory and finish the jobs; windows that reach the
+ * image border, or images not on 16-byte boundaries or with dstride not a
+ * multiple of 4, take the global-memory path).  The CLT is bit-identical to
+ * tp_convert_correct_tiles'.  A bounded wait that runs out leaves the CLT
+ * incomplete and is reported by tp_tc_status. */
+int tp_convert_correct_tiles_tma(const tp_geometry *g, float *const *kernel_offsets, float *const *kernels,
+                                 float *const *images, const tp_task *tasks, float *const *clt, size_t dstride,
+                                 int num_tiles, int lpf_mask, tp_stream_t stream);
 
 /* ---- pairwise phase correlation ---------------------------------------------
  * Replaces correlate2D (src/TileProcessor.cuh:1176-1443).
@@ -543,9 +554,9 @@ int tp_generate_RBGA_tc(const tp_geometry *g,
                         float *const *tile_scratch,
                         int format,
                         tp_stream_t stream);
-/* *timed_out = 1 when a tensor-core stage kernel's wait ran out since the
- * last clear (synchronous); clear != 0 resets it.  No counterpart in the
- * reference. */
+/* *timed_out = 1 when a tensor-core stage kernel's (or the TMA-fed convert
+ * kernel's) wait ran out since the last clear (synchronous); clear != 0
+ * resets it.  No counterpart in the reference. */
 int tp_tc_status(int *timed_out, int clear);
 /* The 64 KB shared-memory image of a stage's split transform matrices
  * (stage 0 correlation, 1 inverse CLT, 2 forward CLT): uint16 halves, the

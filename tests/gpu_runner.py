@@ -54,6 +54,9 @@ def convert(fr, lpf_mask=0, impl="b200", num_tiles=None):
     if impl == "b200":
         api.convert_correct_tiles(fr.g, fr.p_extra, fr.p_kernels, fr.p_images, fr.tasks, fr.p_clt, c.dstride, n,
                                   lpf_mask)
+    elif impl == "tma":
+        api.convert_correct_tiles_tma(fr.g, fr.p_extra, fr.p_kernels, fr.p_images, fr.tasks, fr.p_clt, c.dstride,
+                                      n, lpf_mask)
     elif impl.startswith("tc_"):
         api.convert_correct_tiles_tc(fr.g, fr.p_extra, fr.p_kernels, fr.p_images, fr.tasks, fr.p_clt, c.dstride, n,
                                      lpf_mask, fmt=_tc_fmt(impl))

@@ -113,6 +113,30 @@ def test_convert_lpf_and_partial_lists(frames, oracle):
     assert np.all(b[0][13 * 768:] == 0)
 
 
+@pytest.mark.parametrize("name", list(CASES) + ["D256sparse"])
+def test_convert_tma_matches_plain(frames, clts, name):
+    """tp_convert_correct_tiles_tma (Bayer windows staged in shared memory by
+    the TMA unit's bulk copies, border windows read from global memory) gives
+    the plain kernel's CLT bit for bit, in both border modes and on a sparse
+    task list; with the LPF and with a count that is not a multiple of 4 as
+    well; no wait runs out."""
+    from tile_processor_gpu_b200 import api
+    R = _R()
+    fr = frames[name]
+    api.tc_status(clear=True)
+    t = R.convert(fr, impl="tma")
+    b, _ = clts[name]
+    for cam in range(4):
+        assert np.array_equal(t[cam], b[cam]), cam
+    if name == "A256ref":
+        for kw in (dict(lpf_mask=7), dict(num_tiles=13)):
+            p = R.convert(fr, **kw)
+            t = R.convert(fr, impl="tma", **kw)
+            for cam in range(4):
+                assert np.array_equal(t[cam], p[cam]), (kw, cam)
+    assert api.tc_status() == 0
+
+
 def test_convert_skips_nop_and_out_of_range_tasks(frames, oracle):
     R = _R()
     fr = frames["A256ref"]

@@ -49,6 +49,7 @@ _G = ctypes.POINTER(TpGeometry)
 # name -> argtypes (restype is int for all compute entry points)
 SIGNATURES = {
     "tp_convert_correct_tiles": [_G, _P, _P, _P, _P, _P, _S, _I, _I, _P],
+    "tp_convert_correct_tiles_tma": [_G, _P, _P, _P, _P, _P, _S, _I, _I, _P],
     "tp_correlate2D": [_G, _P, _I, _F, _F, _F, _F, _S, _P, _S, _I, _P, _P],
     "tp_textures_accumulate": [_G, _P, _P, _S, _P, _P, _I, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, _I,
                                _S, _P, _S, _P, _P],

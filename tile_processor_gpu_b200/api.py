@@ -106,6 +106,15 @@ def convert_correct_tiles(geom, gpu_kernel_offsets, gpu_kernels, gpu_images, gpu
                  int(lpf_mask), _stream(stream))
 
 
+def convert_correct_tiles_tma(geom, gpu_kernel_offsets, gpu_kernels, gpu_images, gpu_tasks, gpu_clt, dstride,
+                              num_tiles, lpf_mask=0, stream=None):
+    """convert_correct_tiles with the Bayer windows staged in shared memory by
+    the TMA unit (tp_convert_correct_tiles_tma; the same CLT)."""
+    _native.call("tp_convert_correct_tiles_tma", geom.ptr, _parr(gpu_kernel_offsets), _parr(gpu_kernels),
+                 _parr(gpu_images), _dptr(gpu_tasks), _parr(gpu_clt), int(dstride), int(num_tiles),
+                 int(lpf_mask), _stream(stream))
+
+
 def correlate2D(geom, gpu_clt, colors, scale0, scale1, scale2, fat_zero, num_corr_tiles, gpu_corr_indices,
                 corr_stride, corr_radius, gpu_corrs, stream=None):
     """Pairwise 2-D phase correlation (correlate2D)."""

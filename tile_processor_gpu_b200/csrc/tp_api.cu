@@ -32,6 +32,7 @@
 #include "tp_fwd_tc.cuh"
 #include "tp_mlp.cuh"
 #include "tp_gemm_tc.cuh"
+#include "tp_convert_tma.cuh"
 
 #define TP_VERSION "tile_processor_gpu_b200 0.1 (sm_100a)"
 
@@ -118,7 +119,7 @@ int shape_per_sm(int which)
  * their attribute once per device (the first call; make it before capturing
  * a stream into a graph). */
 std::mutex g_attr_mutex;
-bool g_tex_attr[4][128], g_frame_attr[128], g_tc_attr[128], g_gemm_tc_attr[128];
+bool g_tex_attr[4][128], g_frame_attr[128], g_tc_attr[128], g_gemm_tc_attr[128], g_cv_attr[128];
 
 int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
 {
@@ -1110,6 +1111,30 @@ int tp_tc_status(int *timed_out, int clear)
         if (e != cudaSuccess) return fail(TP_ERR_CUDA, "tensor-core status: %s", cudaGetErrorString(e));
     }
     return TP_OK;
+}
+
+int tp_convert_correct_tiles_tma(const tp_geometry *g, float *const *kernel_offsets, float *const *kernels,
+                                 float *const *images, const tp_task *tasks, float *const *clt, size_t dstride,
+                                 int num_tiles, int lpf_mask, tp_stream_t stream)
+{
+    tp::Geom gd;
+    int rc = check_geometry(g, &gd);
+    if (rc) return rc;
+    if (!kernel_offsets || !kernels || !images || !clt) return fail(TP_ERR_ARG, "NULL pointer array");
+    if (num_tiles < 0) return fail(TP_ERR_ARG, "num_tiles %d < 0", num_tiles);
+    if (num_tiles > 0 && !tasks) return fail(TP_ERR_ARG, "tasks is NULL");
+    if (dstride < (size_t)g->img_width) return fail(TP_ERR_ARG, "dstride %zu < width %d", dstride, g->img_width);
+    if (num_tiles == 0) return TP_OK;
+    int sms, *err;
+    if ((rc = sm_count(&sms)) || (rc = tc_err_ptr(&err))) return rc;
+    if ((rc = set_smem_once(g_cv_attr, (const void *)tp::k_convert_tma, tp::kCvSmemBytes,
+                            "cudaFuncSetAttribute(k_convert_tma)")))
+        return rc;
+    const long long items = (long long)((num_tiles + 3) / 4) * 12;
+    const unsigned grid = grid_for(items, 1, sms, 2);
+    tp::k_convert_tma<<<grid, tp::kCvThreads, tp::kCvSmemBytes, (cudaStream_t)stream>>>(
+        gd, dstride, kernel_offsets, kernels, images, tasks, clt, num_tiles, lpf_mask, err);
+    return cuda_status(cudaGetLastError(), "convert_correct_tiles_tma launch");
 }
 
 int tp_tc_table_image(int format, int stage, void *out)

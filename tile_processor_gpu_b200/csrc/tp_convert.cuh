@@ -86,12 +86,18 @@ __device__ __forceinline__ JobGeometry job_geometry(const Geom &g, const float *
     return j;
 }
 
+/* A job's window staged in shared memory (the TMA-fed convert kernel): 16
+ * rows of 20 floats from the 16-byte boundary at or left of the corner */
+constexpr int kCvWinW = 20, kCvWinH = 16;
+
 /* The fold: lane l builds DTT row l of the folded, windowed Bayer samples of
  * the job's colour (P: the cosine fold; Q: the sine-windowed fold of green,
  * zeros for red and blue), both Bayer phases of green summed
- * (src/TileProcessor.cuh:3257-3416). */
+ * (src/TileProcessor.cuh:3257-3416).  win (may be NULL): the job's window in
+ * shared memory, used for windows inside the image (the same samples). */
 __device__ __forceinline__ void fold_rows(const Geom &g, size_t dstride, const float *__restrict__ img,
-                                          const JobGeometry &j, int color, int l, float P[8], float Q[8])
+                                          const JobGeometry &j, int color, int l, float P[8], float Q[8],
+                                          const float *win = nullptr, int win_dx = 0)
 {
     const int itlx = j.itlx, itly = j.itly;
     const int c0 = color & 1, c1 = (color >> 1) & 1;
@@ -126,7 +132,11 @@ __device__ __forceinline__ void fold_rows(const Geom &g, size_t dstride, const f
             const int lc = fold_sample(v, colp);
             const float whs_raw = shifted_window(lc, j.hc, j.hs);
             float pix;
-            if (fast) {
+            if (fast && win) {
+                /* the window staged in shared memory: rows of kCvWinW floats from
+                 * column itlx - win_dx */
+                pix = win[lr * kCvWinW + win_dx + lc];
+            } else if (fast) {
                 pix = __ldg(img + rowbase + lc);
             } else if (g.border_mode == TP_BORDER_CLAMP) {
                 pix = __ldg(img + rowbase + pair_clamp(itlx + lc, g.W));
@@ -148,6 +158,11 @@ __device__ __forceinline__ void fold_rows(const Geom &g, size_t dstride, const f
  * kernel tiles and Bayer rows that neighbouring jobs of this kernel still
  * read. */
 template <bool STREAM = false>
+__device__ __forceinline__ void convert_finish(const float *__restrict__ kern_tab, const JobGeometry &jg, int color,
+                                               int lpf_mask, float *__restrict__ out, float (*tb)[9], int l,
+                                               unsigned gm, float P[8], float Q[8]);
+
+template <bool STREAM = false>
 __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
                                             const float *__restrict__ extra_tab,
                                             const float *__restrict__ kern_tab,
@@ -156,14 +171,23 @@ __device__ __forceinline__ void convert_job(const Geom &g, size_t dstride,
                                             float (*tb)[9], int l, unsigned gm, const float *pre_ex = nullptr)
 {
     const JobGeometry jg = job_geometry(g, extra_tab, cx, cy, color, pre_ex);
+    /* ---- fold: lane l builds DTT row l ---- */
+    float P[8], Q[8];
+    fold_rows(g, dstride, img, jg, color, l, P, Q);
+    convert_finish<STREAM>(kern_tab, jg, color, lpf_mask, out, tb, l, gm, P, Q);
+}
+
+/* The rest of a job after its fold: 2-D transform, CLT-domain convolution
+ * with the kernel tile, residual shifts, LPF, store. */
+template <bool STREAM>
+__device__ __forceinline__ void convert_finish(const float *__restrict__ kern_tab, const JobGeometry &jg, int color,
+                                               int lpf_mask, float *__restrict__ out, float (*tb)[9], int l,
+                                               unsigned gm, float P[8], float Q[8])
+{
     const size_t kidx = jg.kidx;
     const int itlx = jg.itlx, itly = jg.itly;
     const float shx = jg.shx, shy = jg.shy;
     const int c1 = (color >> 1) & 1;
-
-    /* ---- fold: lane l builds DTT row l ---- */
-    float P[8], Q[8];
-    fold_rows(g, dstride, img, jg, color, l, P, Q);
 
     /* ---- 2-D transform: rows (registers), transpose, columns ---- */
     float cc[8], sc[8], cs[8], ss[8], t[8];
