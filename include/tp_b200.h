@@ -145,6 +145,9 @@ enum {
 int tp_set_launch_shape(int kernel, int ctas_per_sm);
 /* the value in use (the built-in one when unset), TP_ERR_ARG for an unknown kernel */
 int tp_get_launch_shape(int kernel);
+/* how many CTAs of the stage kernel fit on one SM at once (its registers,
+ * block size and shared memory); caps above it only add waves */
+int tp_resident_ctas(int kernel);
 
 /* ---- forward CLT with aberration correction ---------------------------------
  * Replaces convert_correct_tiles (src/TileProcessor.cuh:1859-1937).

@@ -87,6 +87,7 @@ SIGNATURES = {
     "tp_tiles_ya": [_G],
     "tp_set_launch_shape": [_I, _I],
     "tp_get_launch_shape": [_I],
+    "tp_resident_ctas": [_I],
     "tp_correlate2D_tc": [_G, _P, _I, _F, _F, _F, _F, _S, _P, _S, _I, _P, _I, _P],
     "tp_convert_correct_tiles_tc": [_G, _P, _P, _P, _P, _P, _S, _I, _I, _I, _P],
     "tp_textures_accumulate_tc": [_G, _P, _P, _S, _P, _P, _I, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, _I,

@@ -5,7 +5,10 @@ at `ctas_per_sm` x the SM count (tp_set_launch_shape); the cap decides how
 many tiles each CTA takes in turn and how many CTAs share an SM.  The tuner
 times the caller's own workload on the GPU under each candidate cap (CUDA
 events on the current stream, after warm-up runs) and keeps the fastest.
-Shapes are process-wide; a CUDA graph keeps the shapes it was captured with.
+Candidates above the number of CTAs that fit on an SM at once
+(tp_resident_ctas) are dropped: they only run the same blocks in more
+waves.  Shapes are process-wide; a CUDA graph keeps the shapes it was
+captured with.
 """
 from . import _native
 
@@ -13,6 +16,17 @@ KERNELS = {"convert": 0, "correlate": 1, "textures": 2}
 CANDIDATES = {"convert": (2, 3, 4, 6, 8, 12, 16),
               "correlate": (4, 6, 8, 12, 16),
               "textures": (5, 6, 7, 14, 21)}
+
+
+def resident(kernel):
+    """CTAs of the stage kernel that fit on one SM at once"""
+    return _native.call("tp_resident_ctas", KERNELS[kernel])
+
+
+def resident_candidates(kernel):
+    """the built-in candidate caps that fit on an SM at once, and that limit itself"""
+    r = resident(kernel)
+    return tuple(sorted({c for c in CANDIDATES[kernel] if c <= r} | {r}))
 
 
 def set_shape(kernel, ctas_per_sm):
@@ -41,7 +55,7 @@ def time_ms(run, repeats, warmup):
 def tune(kernel, run, candidates=None, repeats=10, warmup=2):
     """Time run() (a workload that launches `kernel`) under each candidate
     cap; leave the fastest set.  Returns (best, {cap: ms})."""
-    cands = tuple(candidates if candidates is not None else CANDIDATES[kernel])
+    cands = tuple(candidates if candidates is not None else resident_candidates(kernel))
     times = {}
     for c in cands:
         set_shape(kernel, c)
@@ -58,7 +72,8 @@ def tune_stages(stages, repeats=10, warmup=2):
     out = {}
     for kernel, run in stages.items():
         best, times = tune(kernel, run, repeats=repeats, warmup=warmup)
-        out[kernel] = {"ctas_per_sm": best, "ms": {str(k): round(v, 4) for k, v in times.items()}}
+        out[kernel] = {"ctas_per_sm": best, "resident": resident(kernel),
+                       "ms": {str(k): round(v, 4) for k, v in times.items()}}
     return out
 
 

@@ -256,6 +256,24 @@ int tp_get_launch_shape(int kernel)
     if (kernel < 0 || kernel >= TP_SHAPE_COUNT) return fail(TP_ERR_ARG, "launch shape kernel %d", kernel);
     return shape_per_sm(kernel);
 }
+
+int tp_resident_ctas(int kernel)
+{
+    if (kernel < 0 || kernel >= TP_SHAPE_COUNT) return fail(TP_ERR_ARG, "launch shape kernel %d", kernel);
+    int n = 0, rc;
+    cudaError_t e;
+    if (kernel == TP_SHAPE_CONVERT) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tp::k_convert_correct_tiles, 256, 0);
+    } else if (kernel == TP_SHAPE_CORRELATE) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tp::k_correlate2D, 128, 0);
+    } else {
+        if ((rc = texture_smem_setup())) return rc;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tp::k_textures<false, false>, tp::kTexThreads,
+                                                          tp::kTexSmemBytes);
+    }
+    if (e != cudaSuccess) return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    return n;
+}
 const char *tp_version(void) { return TP_VERSION; }
 
 int tp_tiles_x(const tp_geometry *g) { return g ? g->img_width / 8 : 0; }
