@@ -137,6 +137,24 @@ def test_convert_tma_matches_plain(frames, clts, name):
     assert api.tc_status() == 0
 
 
+def test_convert_tma_unstaged_pitch(native, oracle):
+    """Rows 4 n + 1 floats apart do not start on 16-byte boundaries: every
+    window of tp_convert_correct_tiles_tma then takes the global-memory path,
+    and the CLT still equals the plain kernel's and the oracle's."""
+    from tile_processor_gpu_b200 import api
+    R = _R()
+    fr = R.Frame(Case(256, 192, seed=12, border_mode=0, pitch_extra=5))
+    c = fr.case
+    assert c.dstride % 4 == 1
+    p = R.convert(fr)
+    t = R.convert(fr, impl="tma")
+    for cam in range(4):
+        assert np.array_equal(t[cam], p[cam]), cam
+    o = oracle.convert_correct_tiles(c.geom, c.extra, c.kernels, c.pitched, c.dstride, c.tasks)
+    assert max(rel_err(t[k], o[k]) for k in range(4)) < TOL
+    assert api.tc_status() == 0
+
+
 def test_convert_skips_nop_and_out_of_range_tasks(frames, oracle):
     R = _R()
     fr = frames["A256ref"]
