@@ -8,7 +8,8 @@ two planes with an occlusion edge, disparity from 0 to 8..64 px across the
 frame, shot noise and a read-noise sigma drawn log-uniformly in
 [0.001, 0.02], seen through one of eight lenses (kernel tables of 256 PSF
 shapes each); its tiles are tasked at the true disparity plus a per-tile
-error U[-e, e] px, e drawn per frame in [0.3, 1.2].  The library's own
+error U[-e, e] px, e drawn per frame in [0.3, 1.2] (--task-error,
+--log-error).  The library's own
 pipeline (forward CLT, pair correlation, plain fit, features) turns each
 frame into samples; the network is trained with its own kernels
 (disparity_net).  Eight validation frames choose the log-variance gate above
@@ -29,11 +30,18 @@ import numpy as np
 W_DEF, H_DEF = 1024, 768
 
 
+# per-frame task-error bound e (px): uniform in [lo, hi], or log-uniform
+TASK_ERROR = {"lo": 0.3, "hi": 1.2, "log": False}
+
+
 def _frame_draws(seed):
     """per-frame disparity span, task error, lens index, scene kind (a third
     of the frames have an occlusion edge) and read-noise sigma (log-uniform)"""
     r = np.random.default_rng(seed + 7_000_001)
-    return (float(r.uniform(8.0, 64.0)), float(r.uniform(0.3, 1.2)), int(r.integers(0, N_LENSES)),
+    span = float(r.uniform(8.0, 64.0))
+    lo, hi = TASK_ERROR["lo"], TASK_ERROR["hi"]
+    e = float(np.exp(r.uniform(np.log(lo), np.log(hi)))) if TASK_ERROR["log"] else float(r.uniform(lo, hi))
+    return (span, e, int(r.integers(0, N_LENSES)),
             "occlusion" if r.uniform() < OCCLUSION_FRACTION else "plane",
             float(np.exp(r.uniform(np.log(0.001), np.log(0.02)))))
 
@@ -127,9 +135,13 @@ def main(argv=None):
     ap.add_argument("--width", type=int, default=W_DEF)
     ap.add_argument("--height", type=int, default=H_DEF)
     ap.add_argument("--workers", type=int, default=max(1, min(16, (os.cpu_count() or 2) - 1)))
+    ap.add_argument("--task-error", default="0.3,1.2", help="per-frame task-error bound range lo,hi (px)")
+    ap.add_argument("--log-error", action="store_true", help="draw the bound log-uniformly in the range")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
                                                   "disparity_mlp.npz"))
     args = ap.parse_args(argv)
+    lo, hi = (float(v) for v in args.task_error.split(","))
+    TASK_ERROR.update(lo=lo, hi=hi, log=bool(args.log_error))
     import torch
     from tile_processor_gpu_b200 import build, disparity_net as D
     build.build()
@@ -160,7 +172,8 @@ def main(argv=None):
     fin = lambda v: v if np.isfinite(v) else None  # noqa: E731  (no gate: null)
     report = {"train_tiles": int(feats.shape[0]), "holdout_tiles": int(hf.shape[0]), "frames": args.frames,
               "holdout_frames": args.holdout, "epochs": args.epochs, "frame": "%dx%d" % (args.width, args.height),
-              "lenses": N_LENSES, "disparity_span_px": [8, 64], "task_error_px": [0.3, 1.2],
+              "lenses": N_LENSES, "disparity_span_px": [8, 64], "task_error_px": [lo, hi],
+              "task_error_draw": "log-uniform" if args.log_error else "uniform",
               "scenes": "slanted planes; a third two planes with an occlusion edge",
               "read_sigma": "log-uniform in [0.001, 0.02]",
               "validation_frames": args.validation, "gate_logvar": fin(net.gate),
