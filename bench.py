@@ -247,16 +247,48 @@ class BatchedFrames:
         self.tiles = sum(f["num_tiles"] for f in self.frames)
         self.pixels = sum(f["size"][0] * f["size"][1] for f in self.frames)
 
-    def run_frame(self, f):
+    def run_frame(self, f, lane=None):
+        """the frame's three calls, on the pipe's buffers or on a lane's (its
+        own CLT, correlation, list and RGBA buffers)"""
         p, api, t = self.pipe, self.api, TEXTURE
-        api.convert_correct_tiles(f["g"], f["p_extra"], f["p_kernels"], f["p_images"], f["tasks"], p.p_clt,
+        b = lane if lane is not None else {"p_clt": p.p_clt, "corrs": p.corrs, "tex_indices": p.tex_indices,
+                                           "num_tex": p.num_tex, "woi": p.woi, "rgba": p.rgba}
+        api.convert_correct_tiles(f["g"], f["p_extra"], f["p_kernels"], f["p_images"], f["tasks"], b["p_clt"],
                                   f["dstride"], f["num_tiles"], 0)
-        api.correlate2D(f["g"], p.p_clt, 3, 0.25, 0.25, 0.5, FAT_ZERO, f["num_corr"], f["corr_idx"], p.corr_stride,
-                        CORR_RADIUS, p.corrs)
-        api.generate_RBGA(f["g"], f["tasks"], f["num_tiles"], p.tex_indices, p.num_tex, p.woi, f["TX"], f["TY"],
-                          p.p_clt, p.port_offsets, t["colors"], t["is_lwir"], t["min_shot"], t["scale_shot"],
-                          t["diff_sigma"], t["diff_threshold"], t["min_agree"], t["weight0"], t["weight1"],
-                          t["weight2"], t["dust_remove"], 0, f["rgba_stride"], p.rgba)
+        api.correlate2D(f["g"], b["p_clt"], 3, 0.25, 0.25, 0.5, FAT_ZERO, f["num_corr"], f["corr_idx"],
+                        p.corr_stride, CORR_RADIUS, b["corrs"])
+        api.generate_RBGA(f["g"], f["tasks"], f["num_tiles"], b["tex_indices"], b["num_tex"], b["woi"], f["TX"],
+                          f["TY"], b["p_clt"], p.port_offsets, t["colors"], t["is_lwir"], t["min_shot"],
+                          t["scale_shot"], t["diff_sigma"], t["diff_threshold"], t["min_agree"], t["weight0"],
+                          t["weight1"], t["weight2"], t["dust_remove"], 0, f["rgba_stride"], b["rgba"])
+
+    def lanes(self, count):
+        """`count` buffer sets for frames in flight on separate streams, and
+        the frames' lanes: the largest frame first to the lane with the
+        fewest tiles so far"""
+        torch, p, api = self.pipe.torch, self.pipe, self.api
+        out = []
+        for _ in range(count):
+            clt = [torch.empty_like(c) for c in p.clt]
+            out.append({"clt": clt, "p_clt": api.PointerArray(clt), "corrs": torch.empty_like(p.corrs),
+                        "tex_indices": torch.empty_like(p.tex_indices), "num_tex": torch.empty_like(p.num_tex),
+                        "woi": torch.empty_like(p.woi), "rgba": torch.empty_like(p.rgba)})
+        load, assign = [0] * count, [0] * len(self.frames)
+        for i in sorted(range(len(self.frames)), key=lambda i: -self.frames[i]["num_tiles"]):
+            k = min(range(count), key=lambda j: load[j])
+            assign[i] = k
+            load[k] += self.frames[i]["num_tiles"]
+        return out, assign
+
+    def run_streams(self, origin, streams, lanes, assign):
+        """every frame on its lane's stream, forked from and joined back to `origin`"""
+        for s in streams:
+            s.wait_stream(origin)
+        for f, k in zip(self.frames, assign):
+            with self.pipe.torch.cuda.stream(streams[k]):
+                self.run_frame(f, lanes[k])
+        for s in streams:
+            origin.wait_stream(s)
 
     def run_all(self):
         for f in self.frames:
@@ -293,6 +325,26 @@ class BatchedFrames:
         torch.cuda.synchronize()
         graph_ms = g0.elapsed_time(g1) / replays
         del graph
+        # the same frames on four streams (own buffers per stream), one graph
+        nlanes = 4
+        lanes, assign = self.lanes(nlanes)
+        streams = [torch.cuda.Stream() for _ in range(nlanes)]
+        self.run_streams(stream, streams, lanes, assign)
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(graph, stream=side):
+                self.run_streams(side, streams, lanes, assign)
+        stream.wait_stream(side)
+        graph.replay()
+        torch.cuda.synchronize()
+        g0.record(stream)
+        for _ in range(replays):
+            graph.replay()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        streams_ms = g0.elapsed_time(g1) / replays
+        del graph, lanes
         n = len(self.frames)
         return {"frames": n, "sizes": "%dx%d .. %dx%d" % (min(f["size"][0] for f in self.frames),
                                                          min(f["size"][1] for f in self.frames),
@@ -306,7 +358,15 @@ class BatchedFrames:
                 "frame_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
                              "p99": round(float(np.percentile(lat, 99)), 4),
                              "max": round(float(lat.max()), 4)},
-                "full_frame_equivalent_per_s": round(self.tiles / (self.pipe.TX * self.pipe.TY) / graph_ms * 1e3, 1)}
+                "full_frame_equivalent_per_s": round(self.tiles / (self.pipe.TX * self.pipe.TY) / graph_ms * 1e3, 1),
+                "streams": {"count": nlanes, "what": "the same frames on %d streams (each with its own CLT, "
+                            "correlation, list and RGBA buffers; frames to the stream with the fewest tiles, "
+                            "largest first), forked and joined inside one CUDA graph" % nlanes,
+                            "graph_ms_per_batch": round(streams_ms, 3),
+                            "frames_per_s": round(n / streams_ms * 1e3, 1),
+                            "tiles_per_s": round(self.tiles / streams_ms * 1e3, 0),
+                            "full_frame_equivalent_per_s": round(
+                                self.tiles / (self.pipe.TX * self.pipe.TY) / streams_ms * 1e3, 1)}}
 
 
 # --------------------------------------------------------------------------- #
