@@ -70,7 +70,8 @@ __global__ void __launch_bounds__(kFrameThreads, kFrameBlocksPerSm) k_frame(
     const int tid = threadIdx.x;
     const int l = tid & 7, grp = tid >> 3;
     const unsigned gm = group_mask();
-    const float ksigma = (float)(1.0 / (2.0 * (double)p.tex.diff_sigma * (double)p.tex.diff_sigma));
+    /* 1 / (2 sigma^2) times log2(e), as combine_pixel takes it */
+    const float ksigma = (float)(1.0 / (2.0 * (double)p.tex.diff_sigma * (double)p.tex.diff_sigma)) * kLog2e;
     if (tid == 0) {
         int k = 0;
         for (int i = 0; i < 4; i++)

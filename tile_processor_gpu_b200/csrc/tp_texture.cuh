@@ -187,11 +187,25 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
     __syncwarp(gm);
 }
 
+/* log2(e): e^x = 2^(x log2 e) */
+constexpr float kLog2e = 1.4426950408889634f;
+
+/* 2^x from the hardware's base-2 exponential (PTX ex2.approx.ftz; results
+ * below the smallest normal float flush to zero) */
+__device__ __forceinline__ float exp2_hw(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 /* Fuse the four cameras at one pixel (tile_combine_rgba, one pixel).
  * sd: debayered tiles D; sm: the plain (not debayered) tiles, scaled by
  * m_scale (the plain tile is the un-windowed one times the squared window);
  * both [job = cam * colors + color] with the given strides, pixel offset e.
- * chw: the colour weights; chws: their square roots.
+ * chw: the colour weights; chws: their square roots.  pd2r (the six pairs'
+ * 1 / (2 sigma^2 |offset|^2)) and ksigma (1 / (2 sigma^2)) come multiplied by
+ * log2(e): each weight exp(-k d) is evaluated as 2^(-(k log2 e) d).
  * o: colours, alpha, 4 port weights and (keep_weights) colors + 1 rms.
  * The colour distances sum_col chw[col] ((X[col] - Y[col]) wi)^2 are formed
  * as sum_col (X'[col] - Y'[col])^2 in the scaled space X' = X wi sqrt(chw),
@@ -240,9 +254,10 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
      * is tiny (high-contrast or high-dynamic-range tiles), and a float sum
      * with 1e-4f can land one ulp lower and break such ties the other way
      * (splitting the floor into two floats still rounds 1 in 2e6 tiny sums
-     * differently).  The exponential itself is the hardware one: its
-     * relative error (below 1e-6 wherever a weight is above the floor) is
-     * under what float32 inputs already move it by. */
+     * differently).  The exponential is the hardware's base-2 one with the
+     * log2(e) factor folded into pd2r and ksigma: its relative error (about
+     * 2^-22) is under what float32 inputs already move a weight by, and a
+     * flushed subnormal weight is lost in the 1e-4 floor. */
     float pw[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     {
         int k = 0;
@@ -256,7 +271,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
                     const float dc = D[i][col] - D[j][col];
                     d = __fmaf_rn(dc, dc, d);
                 }
-                const float x = __double2float_rn((double)__expf(-pd2r[k] * d) + 1e-4);
+                const float x = __double2float_rn((double)exp2_hw(-pd2r[k] * d) + 1e-4);
                 pw[i] += x;
                 pw[j] += x;
                 k++;
@@ -296,7 +311,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
             const float dc = D[cam][col] - avg[col];
             d2 = __fmaf_rn(dc, dc, d2);
         }
-        pw[cam] = __double2float_rn((double)__expf(-ksigma * d2) + 1e-4);
+        pw[cam] = __double2float_rn((double)exp2_hw(-ksigma * d2) + 1e-4);
     }
     if (dust_remove) {
         int worst = 0;
@@ -363,7 +378,8 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     const unsigned gm = group_mask();
     const int colors = p.colors;
     const int njobs = 4 * colors;
-    const float ksigma = (float)(1.0 / (2.0 * (double)p.diff_sigma * (double)p.diff_sigma));
+    /* 1 / (2 sigma^2) times log2(e): the fusion's weights are powers of two */
+    const float ksigma = (float)(1.0 / (2.0 * (double)p.diff_sigma * (double)p.diff_sigma)) * kLog2e;
     if (tid < 4) s_cp[tid] = clt[tid];
     if (tid == 0) {
         int k = 0;
