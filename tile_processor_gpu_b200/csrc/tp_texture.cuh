@@ -146,7 +146,6 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
      * squared window of an unrolled row folds into an immediate operand */
     constexpr float kHwin[16] = TP_HWIN_INIT;
     __syncwarp(gm);
-    const float kshot = rsqrtf(min_shot);
     const bool shot = scale_shot > 0.0f;
     const float kdiag = rb_mode ? 0.0625f : 0.0f, kcenter = rb_mode ? 0.25f : 0.5f;
 #pragma unroll
@@ -177,10 +176,11 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
                 a1 = b1; ha = hb;
                 b1 = e1; hb = he;
             }
-            /* shot-noise square root above min_shot: v / sqrt(v) from the
-             * hardware reciprocal square root (within 3e-7 of sqrtf), cheap
-             * enough to evaluate on both sides of the select */
-            if (shot) v = (v > min_shot) ? v * rsqrtf(fmaxf(v, 1e-30f)) : (kshot * v);
+            /* shot-noise square root above min_shot, v / sqrt(min_shot) at or
+             * below it: both are v * rsqrt(max(v, min_shot)) (min_shot > 0
+             * whenever the transform applies), from the hardware reciprocal
+             * square root (within 3e-7 of sqrtf) */
+            if (shot) v = v * rsqrtf(fmaxf(v, min_shot));
             d[JT(r, c)] = v * (swx * (kHwin[r] * kHwin[r]));
         }
     }
