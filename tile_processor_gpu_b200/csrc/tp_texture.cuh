@@ -138,9 +138,12 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
  * that use it; red/blue (rb_mode) and green take one branch-free form (the
  * diagonal term's weight is 0 for green), so the groups of a warp, which
  * hold different colours, do not diverge; the shot-noise scale and the two
- * window factors are one product per pixel. */
+ * window factors are one product per pixel.  windowed = false stores D
+ * without them (the camera fusion of the RGBA-only path measures distances
+ * in D wi sqrt(w) scale_shot, where the squared window cancels against wi =
+ * 1 / wnd2: it takes scale_shot with its colour factors instead). */
 __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mode, float min_shot,
-                                            float scale_shot, int l, unsigned gm)
+                                            float scale_shot, int l, unsigned gm, bool windowed = true)
 {
     /* the window as compile-time constants (the values of c_hwin): the
      * squared window of an unrolled row folds into an immediate operand */
@@ -181,7 +184,7 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
              * whenever the transform applies), from the hardware reciprocal
              * square root (within 3e-7 of sqrtf) */
             if (shot) v = v * rsqrtf(fmaxf(v, min_shot));
-            d[JT(r, c)] = v * (swx * (kHwin[r] * kHwin[r]));
+            d[JT(r, c)] = windowed ? v * (swx * (kHwin[r] * kHwin[r])) : v;
         }
     }
     __syncwarp(gm);
@@ -203,7 +206,9 @@ __device__ __forceinline__ float exp2_hw(float x)
  * sd: debayered tiles D; sm: the plain (not debayered) tiles, scaled by
  * m_scale (the plain tile is the un-windowed one times the squared window);
  * both [job = cam * colors + color] with the given strides, pixel offset e.
- * chw: the colour weights; chws: their square roots.  pd2r (the six pairs'
+ * chw: the colour weights; chws: their square roots, times scale_shot when
+ * the D tiles come without the window and the shot scale (d_windowed false;
+ * wi is then not applied to them).  pd2r (the six pairs'
  * 1 / (2 sigma^2 |offset|^2)) and ksigma (1 / (2 sigma^2)) come multiplied by
  * log2(e): each weight exp(-k d) is evaluated as 2^(-(k log2 e) d).
  * o: colours, alpha, 4 port weights and (keep_weights) colors + 1 rms.
@@ -214,7 +219,7 @@ template <int COLORS>
 __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, const float *sm, int sm_stride,
                                               float m_scale, int e, const float *pd2r, float ksigma,
                                               const float *chw, const float *chws, float wnd2, float wi,
-                                              int dust_remove, int keep_weights, float *o)
+                                              int dust_remove, int keep_weights, float *o, bool d_windowed = true)
 {
     float D[4][COLORS];
 #pragma unroll
@@ -243,7 +248,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
     /* D in the scaled space */
 #pragma unroll
     for (int col = 0; col < COLORS; col++) {
-        const float sc = wi * chws[col];
+        const float sc = d_windowed ? wi * chws[col] : chws[col];
 #pragma unroll
         for (int cam = 0; cam < 4; cam++) D[cam][col] *= sc;
     }
@@ -390,8 +395,14 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
                 s_pd2r[k++] = ksigma / (dx * dx + dy * dy);
             }
         s_chw[0] = p.w0; s_chw[1] = p.w1; s_chw[2] = p.w2;
-        for (int c = 0; c < 3; c++) s_chws[c] = sqrtf(s_chw[c]);
+        /* the RGBA-only colour path debayers without the window (see
+         * debayer_job): its distance factors carry the shot scale */
+        const float dsc = (!ALL && p.colors == 3 && p.scale_shot > 0.0f) ? p.scale_shot : 1.0f;
+        for (int c = 0; c < 3; c++) s_chws[c] = sqrtf(s_chw[c]) * dsc;
     }
+    /* D tiles with the window and the shot scale (the keep-weights
+     * statistics and mono need them as the reference forms them) */
+    const bool d_windowed = ALL || p.colors != 3;
 
     long long count = num_texture_tiles;
     const int *lst = list;
@@ -519,7 +530,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
 #pragma unroll
                 for (int c = 0; c < 16; c++) tj[JT(2 * l + h, c)] = v[c];
             }
-            if (colors > 1) debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
+            if (colors > 1) debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm, d_windowed);
         } else if (grp < njobs) {
             const int cam = grp / colors, color = grp - cam * colors;
             float *tj = s_t + grp * kJob, *xj = s_x + grp * kTB4;
@@ -528,7 +539,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
                  * buffer, free once the unfold has read it) */
                 imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[color], xj, nullptr, tj, l,
                                  gm);
-                debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
+                debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm, d_windowed);
             } else {
                 imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[3], xj, tj, nullptr, l, gm);
             }
@@ -561,7 +572,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
             float o[12];
             if (colors == 3)
                 combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
-                                 p.dust_remove, keep_weights, o);
+                                 p.dust_remove, keep_weights, o, d_windowed);
             else
                 combine_pixel<1>(s_t, kJob, s_t, kJob, 1.0f, e, s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
                                  p.dust_remove, keep_weights, o);
