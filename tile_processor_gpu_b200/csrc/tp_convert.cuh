@@ -129,8 +129,15 @@ __device__ __forceinline__ void fold_rows(const Geom &g, size_t dstride, const f
         }
 #pragma unroll
         for (int v = 0; v < 8; v++) {
-            const int lc = fold_sample(v, colp);
-            const float whs_raw = shifted_window(lc, j.hc, j.hs);
+            /* the sample's column for either Bayer phase and its window values
+             * are compile-time constants; the job's phase selects one (the
+             * groups of a warp hold jobs of either phase, so a table indexed
+             * by the run-time column would serialise their reads) */
+            constexpr float kW[16] = TP_HWIN_INIT, kWc[16] = TP_HWINC_INIT;
+            const int lc0 = fold_sample(v, 0), lc1 = fold_sample(v, 1);
+            const int lc = colp ? lc1 : lc0;
+            const float ww = colp ? kW[lc1] : kW[lc0], wwc = colp ? kWc[lc1] : kWc[lc0];
+            const float whs_raw = __fmaf_rn(ww, j.hc, wwc * j.hs);
             float pix;
             if (fast && win) {
                 /* the window staged in shared memory: rows of kCvWinW floats from
@@ -146,8 +153,10 @@ __device__ __forceinline__ void fold_rows(const Geom &g, size_t dstride, const f
                 pix = __ldg(img + a);
             }
             const float d = pix * wv;
-            P[v] = __fmaf_rn(d, fold_sign_c(lc) * whs_raw, P[v]);
-            if (c1) Q[v] = __fmaf_rn(d, fold_sign_s(lc) * whs_raw, Q[v]);
+            const float sgn_c = colp ? fold_sign_c(lc1) : fold_sign_c(lc0);
+            const float sgn_s = colp ? fold_sign_s(lc1) : fold_sign_s(lc0);
+            P[v] = __fmaf_rn(d, sgn_c * whs_raw, P[v]);
+            if (c1) Q[v] = __fmaf_rn(d, sgn_s * whs_raw, Q[v]);
         }
     }
 }
