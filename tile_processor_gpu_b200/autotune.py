@@ -5,10 +5,11 @@ at `ctas_per_sm` x the SM count (tp_set_launch_shape); the cap decides how
 many tiles each CTA takes in turn and how many CTAs share an SM.  The tuner
 times the caller's own workload on the GPU under each candidate cap (CUDA
 events on the current stream, after warm-up runs) and keeps the fastest.
-Candidates above the number of CTAs that fit on an SM at once
-(tp_resident_ctas) are dropped: they only run the same blocks in more
-waves.  Shapes are process-wide; a CUDA graph keeps the shapes it was
-captured with.
+The number of CTAs that fit on an SM at once (tp_resident_ctas) is reported
+beside the timings: caps above it run the extra blocks as they free up, which
+for the forward transform still helps (its blocks' work is uneven) and for
+the texture kernel changes nothing.  Shapes are process-wide; a CUDA graph
+keeps the shapes it was captured with.
 """
 from . import _native
 
@@ -21,12 +22,6 @@ CANDIDATES = {"convert": (2, 3, 4, 6, 8, 12, 16),
 def resident(kernel):
     """CTAs of the stage kernel that fit on one SM at once"""
     return _native.call("tp_resident_ctas", KERNELS[kernel])
-
-
-def resident_candidates(kernel):
-    """the built-in candidate caps that fit on an SM at once, and that limit itself"""
-    r = resident(kernel)
-    return tuple(sorted({c for c in CANDIDATES[kernel] if c <= r} | {r}))
 
 
 def set_shape(kernel, ctas_per_sm):
@@ -55,7 +50,7 @@ def time_ms(run, repeats, warmup):
 def tune(kernel, run, candidates=None, repeats=10, warmup=2):
     """Time run() (a workload that launches `kernel`) under each candidate
     cap; leave the fastest set.  Returns (best, {cap: ms})."""
-    cands = tuple(candidates if candidates is not None else resident_candidates(kernel))
+    cands = tuple(candidates if candidates is not None else CANDIDATES[kernel])
     times = {}
     for c in cands:
         set_shape(kernel, c)
