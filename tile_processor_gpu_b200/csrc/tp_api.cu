@@ -10,6 +10,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <float.h>
 #include <limits.h>
 #include <math.h>
 #include <atomic>
@@ -359,7 +360,9 @@ static int texture_params(int colors, float min_shot, float scale_shot, float di
     if (scale_shot > 0.0f && !(min_shot > 0.0f))
         return fail(TP_ERR_ARG, "min_shot %g must be > 0 when scale_shot > 0", (double)min_shot);
     p->colors = colors;
-    p->min_shot = min_shot;
+    /* the debayer's reciprocal square root takes max(v, min_shot) as a
+     * normal float: a positive min_shot below FLT_MIN acts as FLT_MIN */
+    p->min_shot = (min_shot > 0.0f && min_shot < FLT_MIN) ? FLT_MIN : min_shot;
     p->scale_shot = scale_shot;
     p->diff_sigma = diff_sigma;
     p->w0 = w0;

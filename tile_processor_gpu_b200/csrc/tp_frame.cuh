@@ -81,8 +81,8 @@ __global__ void __launch_bounds__(kFrameThreads, kFrameBlocksPerSm) k_frame(
                 s_pd2r[k++] = ksigma / (dx * dx + dy * dy);
             }
         s_chw[0] = p.tex.w0; s_chw[1] = p.tex.w1; s_chw[2] = p.tex.w2;
-        /* D without the window and the shot scale (debayer_job windowed =
-         * false): the distance factors carry the shot scale */
+        /* D without the window and the shot scale (debayer_job<false>): the
+         * distance factors carry the shot scale */
         const float dsc = p.tex.scale_shot > 0.0f ? p.tex.scale_shot : 1.0f;
         for (int c = 0; c < 3; c++) s_chws[c] = sqrtf(s_chw[c]) * dsc;
     }
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(kFrameThreads, kFrameBlocksPerSm) k_frame(
                 const int color = grp % 3;
                 float *cj = s_clt + grp * kJob, *xj = s_x + grp * kTB4;
                 imclt_unfold_job(cj, d_lpf[color], xj, nullptr, cj, l, gm);
-                debayer_job(cj, xj, color < 2, p.tex.min_shot, p.tex.scale_shot, l, gm, false);
+                debayer_job<false>(cj, xj, color < 2, p.tex.min_shot, p.tex.scale_shot, l, gm);
             }
             __syncthreads();
             prefetch_window();
@@ -235,8 +235,8 @@ __global__ void __launch_bounds__(kFrameThreads, kFrameBlocksPerSm) k_frame(
                     for (int sl = 0; sl < 4; sl++) old[sl] = b[(size_t)sl * slice_stride];
                 }
                 float o[12];
-                combine_pixel<3>(s_x, kTB4, s_clt, kJob, wnd2, JT(r, c), s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
-                                 p.tex.dust_remove, 0, o, false);
+                combine_pixel<3, false>(s_x, kTB4, s_clt, kJob, wnd2, JT(r, c), s_pd2r, ksigma, s_chw, s_chws, wnd2,
+                                        wi, p.tex.dust_remove, 0, o);
                 if (!b) continue;
                 const float f = (nbr != TP_TASK_TEXTURE_BITS) ? __ldg(&d_alpha_fade[nbr][px]) : 1.0f;
 #pragma unroll

@@ -130,6 +130,24 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
     }
 }
 
+/* 1 / sqrt(x) from the hardware's reciprocal square root (PTX
+ * rsqrt.approx.ftz; x must be a normal float or zero) */
+__device__ __forceinline__ float rsqrt_hw(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+/* 1 / x from the hardware's reciprocal (PTX rcp.approx.ftz, within one ulp
+ * of the correctly rounded value for normal x) */
+__device__ __forceinline__ float rcp_hw(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 /* 3x3 debayer of the un-windowed tile T (interior 14x14; border copied),
  * shot-noise square root, squared window re-applied: T -> D
  * (debayer_shot / debayer, :4019-4199).  Lane l: columns l and l + 8, each
@@ -137,13 +155,16 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
  * t[r][c-1] + t[r][c+1] is summed once per row and shared by the three rows
  * that use it; red/blue (rb_mode) and green take one branch-free form (the
  * diagonal term's weight is 0 for green), so the groups of a warp, which
- * hold different colours, do not diverge; the shot-noise scale and the two
- * window factors are one product per pixel.  windowed = false stores D
+ * hold different colours, do not diverge; the border columns (copied
+ * unchanged) take the same form with stencil weights 0, 0 and 1.  The
+ * shot-noise scale and the two window factors are one product per pixel.
+ * WINDOWED = false stores D
  * without them (the camera fusion of the RGBA-only path measures distances
  * in D wi sqrt(w) scale_shot, where the squared window cancels against wi =
  * 1 / wnd2: it takes scale_shot with its colour factors instead). */
+template <bool WINDOWED>
 __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mode, float min_shot,
-                                            float scale_shot, int l, unsigned gm, bool windowed = true)
+                                            float scale_shot, int l, unsigned gm)
 {
     /* the window as compile-time constants (the values of c_hwin): the
      * squared window of an unrolled row folds into an immediate operand */
@@ -156,6 +177,8 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
         const int c = l + 8 * h;
         const bool cborder = (c == 0) || (c == 15);
         const int cm = cborder ? c : c - 1, cp = cborder ? c : c + 1;
+        /* per-lane stencil weights: diagonal, orthogonal, centre */
+        const float kd = cborder ? 0.0f : kdiag, ko = cborder ? 0.0f : 0.125f, kc = cborder ? 1.0f : kcenter;
         const float hcc = __ldg(&d_hwin[c]);
         const float swx = (shot ? scale_shot : 1.0f) * (hcc * hcc);
         float a1 = t[JT(0, c)], ha = t[JT(0, cm)] + t[JT(0, cp)];
@@ -169,22 +192,18 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
                 v = b1;
             } else {
                 const float e1 = t[JT(r + 1, c)], he = t[JT(r + 1, cm)] + t[JT(r + 1, cp)];
-                if (cborder) {
-                    v = b1;
-                } else {
-                    const float orth = (a1 + e1) + hb;
-                    const float diag = ha + he;
-                    v = __fmaf_rn(kdiag, diag, __fmaf_rn(0.125f, orth, kcenter * b1));
-                }
+                const float orth = (a1 + e1) + hb;
+                const float diag = ha + he;
+                v = __fmaf_rn(kd, diag, __fmaf_rn(ko, orth, kc * b1));
                 a1 = b1; ha = hb;
                 b1 = e1; hb = he;
             }
             /* shot-noise square root above min_shot, v / sqrt(min_shot) at or
-             * below it: both are v * rsqrt(max(v, min_shot)) (min_shot > 0
-             * whenever the transform applies), from the hardware reciprocal
-             * square root (within 3e-7 of sqrtf) */
-            if (shot) v = v * rsqrtf(fmaxf(v, min_shot));
-            d[JT(r, c)] = windowed ? v * (swx * (kHwin[r] * kHwin[r])) : v;
+             * below it: both are v * rsqrt(max(v, min_shot)) (min_shot is a
+             * normal float > 0 whenever the transform applies), from the
+             * hardware reciprocal square root (within 3e-7 of sqrtf) */
+            if (shot) v = v * rsqrt_hw(fmaxf(v, min_shot));
+            d[JT(r, c)] = WINDOWED ? v * (swx * (kHwin[r] * kHwin[r])) : v;
         }
     }
     __syncwarp(gm);
@@ -207,7 +226,7 @@ __device__ __forceinline__ float exp2_hw(float x)
  * m_scale (the plain tile is the un-windowed one times the squared window);
  * both [job = cam * colors + color] with the given strides, pixel offset e.
  * chw: the colour weights; chws: their square roots, times scale_shot when
- * the D tiles come without the window and the shot scale (d_windowed false;
+ * the D tiles come without the window and the shot scale (D_WINDOWED false;
  * wi is then not applied to them).  pd2r (the six pairs'
  * 1 / (2 sigma^2 |offset|^2)) and ksigma (1 / (2 sigma^2)) come multiplied by
  * log2(e): each weight exp(-k d) is evaluated as 2^(-(k log2 e) d).
@@ -215,11 +234,11 @@ __device__ __forceinline__ float exp2_hw(float x)
  * The colour distances sum_col chw[col] ((X[col] - Y[col]) wi)^2 are formed
  * as sum_col (X'[col] - Y'[col])^2 in the scaled space X' = X wi sqrt(chw),
  * the same quantity with fewer operations per camera pair. */
-template <int COLORS>
+template <int COLORS, bool D_WINDOWED = true>
 __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, const float *sm, int sm_stride,
                                               float m_scale, int e, const float *pd2r, float ksigma,
                                               const float *chw, const float *chws, float wnd2, float wi,
-                                              int dust_remove, int keep_weights, float *o, bool d_windowed = true)
+                                              int dust_remove, int keep_weights, float *o)
 {
     float D[4][COLORS];
 #pragma unroll
@@ -248,7 +267,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
     /* D in the scaled space */
 #pragma unroll
     for (int col = 0; col < COLORS; col++) {
-        const float sc = d_windowed ? wi * chws[col] : chws[col];
+        const float sc = D_WINDOWED ? wi * chws[col] : chws[col];
 #pragma unroll
         for (int cam = 0; cam < 4; cam++) D[cam][col] *= sc;
     }
@@ -328,7 +347,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
 #pragma unroll
         for (int cam = 0; cam < 4; cam++) a += pw[cam];
         a *= (1.0f / 3.0f);
-        const float ra = __frcp_rn(a);
+        const float ra = rcp_hw(a);
         const float scale = 1.0f + (wv * (a - wv)) * (ra * ra) * (1.0f / 3.0f);
         const float fw = wv * ra;
 #pragma unroll
@@ -337,7 +356,7 @@ __device__ __forceinline__ void combine_pixel(const float *sd, int sd_stride, co
     float ksum = 0.0f;
 #pragma unroll
     for (int cam = 0; cam < 4; cam++) ksum += pw[cam];
-    const float kinv = __frcp_rn(ksum);
+    const float kinv = rcp_hw(ksum);
     float kw[4];
 #pragma unroll
     for (int cam = 0; cam < 4; cam++) kw[cam] = kinv * pw[cam];
@@ -400,9 +419,9 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
         const float dsc = (!ALL && p.colors == 3 && p.scale_shot > 0.0f) ? p.scale_shot : 1.0f;
         for (int c = 0; c < 3; c++) s_chws[c] = sqrtf(s_chw[c]) * dsc;
     }
-    /* D tiles with the window and the shot scale (the keep-weights
-     * statistics and mono need them as the reference forms them) */
-    const bool d_windowed = ALL || p.colors != 3;
+    /* D tiles come with the window and the shot scale in the ALL form and
+     * for mono (the keep-weights statistics and mono need them as the
+     * reference forms them); the RGBA-only colour form debayers without them */
 
     long long count = num_texture_tiles;
     const int *lst = list;
@@ -530,7 +549,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
 #pragma unroll
                 for (int c = 0; c < 16; c++) tj[JT(2 * l + h, c)] = v[c];
             }
-            if (colors > 1) debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm, d_windowed);
+            if (colors > 1) debayer_job<ALL>(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
         } else if (grp < njobs) {
             const int cam = grp / colors, color = grp - cam * colors;
             float *tj = s_t + grp * kJob, *xj = s_x + grp * kTB4;
@@ -539,7 +558,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
                  * buffer, free once the unfold has read it) */
                 imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[color], xj, nullptr, tj, l,
                                  gm);
-                debayer_job(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm, d_windowed);
+                debayer_job<ALL>(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
             } else {
                 imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[3], xj, tj, nullptr, l, gm);
             }
@@ -571,8 +590,8 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
             }
             float o[12];
             if (colors == 3)
-                combine_pixel<3>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
-                                 p.dust_remove, keep_weights, o, d_windowed);
+                combine_pixel<3, ALL>(s_x, kTB4, s_t, kJob, wnd2, e, s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
+                                      p.dust_remove, keep_weights, o);
             else
                 combine_pixel<1>(s_t, kJob, s_t, kJob, 1.0f, e, s_pd2r, ksigma, s_chw, s_chws, wnd2, wi,
                                  p.dust_remove, keep_weights, o);
