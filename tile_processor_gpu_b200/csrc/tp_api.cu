@@ -120,7 +120,7 @@ int shape_per_sm(int which)
  * their attribute once per device (the first call; make it before capturing
  * a stream into a graph). */
 std::mutex g_attr_mutex;
-bool g_tex_attr[4][128], g_frame_attr[128], g_tc_attr[128], g_gemm_tc_attr[128], g_cv_attr[128];
+bool g_tex_attr[8][128], g_frame_attr[128], g_tc_attr[128], g_gemm_tc_attr[128], g_cv_attr[128];
 
 int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
 {
@@ -136,19 +136,23 @@ int set_smem_once(bool *done, const void *func, size_t bytes, const char *what)
     return rc;
 }
 
+/* the texture kernel for a colour count (1 or 3, checked by the caller) */
+template <bool FROM_T, bool ALL>
+static auto tex_kernel(int colors)
+{
+    return colors == 3 ? tp::k_textures<FROM_T, ALL, 3> : tp::k_textures<FROM_T, ALL, 1>;
+}
+
 int texture_smem_setup()
 {
-    int rc = set_smem_once(g_tex_attr[0], (const void *)tp::k_textures<false, true>, tp::kTexSmemBytes,
-                           "cudaFuncSetAttribute(k_textures)");
-    if (!rc)
-        rc = set_smem_once(g_tex_attr[1], (const void *)tp::k_textures<true, true>, tp::kTexSmemBytes,
-                           "cudaFuncSetAttribute(k_textures<tiles>)");
-    if (!rc)
-        rc = set_smem_once(g_tex_attr[2], (const void *)tp::k_textures<false, false>, tp::kTexSmemBytes,
-                           "cudaFuncSetAttribute(k_textures<RGBA>)");
-    if (!rc)
-        rc = set_smem_once(g_tex_attr[3], (const void *)tp::k_textures<true, false>, tp::kTexSmemBytes,
-                           "cudaFuncSetAttribute(k_textures<tiles, RGBA>)");
+    const void *const kernels[8] = {
+        (const void *)tp::k_textures<false, true, 1>,  (const void *)tp::k_textures<false, true, 3>,
+        (const void *)tp::k_textures<true, true, 1>,   (const void *)tp::k_textures<true, true, 3>,
+        (const void *)tp::k_textures<false, false, 1>, (const void *)tp::k_textures<false, false, 3>,
+        (const void *)tp::k_textures<true, false, 1>,  (const void *)tp::k_textures<true, false, 3>};
+    int rc = TP_OK;
+    for (int i = 0; i < 8 && !rc; i++)
+        rc = set_smem_once(g_tex_attr[i], kernels[i], tp::kTexSmemBytes, "cudaFuncSetAttribute(k_textures)");
     return rc;
 }
 
@@ -269,7 +273,7 @@ int tp_resident_ctas(int kernel)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tp::k_correlate2D, 128, 0);
     } else {
         if ((rc = texture_smem_setup())) return rc;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tp::k_textures<false, false>, tp::kTexThreads,
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tp::k_textures<false, false, 3>, tp::kTexThreads,
                                                           tp::kTexSmemBytes);
     }
     if (e != cudaSuccess) return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -400,7 +404,7 @@ int tp_textures_accumulate(const tp_geometry *g, const int *woi, float *const *c
     if ((rc = sm_count(&sms))) return rc;
     if ((rc = texture_smem_setup())) return rc;
     unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
-    tp::k_textures<false, true><<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
+    tex_kernel<false, true>(colors)<<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
         gd, woi, clt, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
         want_tiles ? texture_tiles : nullptr);
@@ -587,18 +591,13 @@ static int generate_rbga(const tp_geometry *g, tp_task *tasks, int num_tiles, in
     /* one pass per tile parity: its inner sub-list, then its border one (the
      * reference runs the four inner passes, then the four border passes;
      * tiles of one parity never overlap, so a pass needs no ordering) */
+    const auto tex = format >= 0 ? tex_kernel<true, false>(colors) : tex_kernel<false, false>(colors);
     for (int parity = 0; parity < 4; parity++) {
         const int *base = texture_indices + parity * quarter;
         const cudaError_t err =
-            format >= 0
-                ? launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures<true, false>, gd,
-                                 (const int *)woi, src, 0LL, (const int *)base, (const int *)num_texture_tiles,
-                                 parity << 1, quarter, -quarter, port_offsets, p, texture_rbga_stride, texture_tiles,
-                                 (size_t)0, (float *)nullptr)
-                : launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tp::k_textures<false, false>, gd,
-                                 (const int *)woi, src, 0LL, (const int *)base, (const int *)num_texture_tiles,
-                                 parity << 1, quarter, -quarter, port_offsets, p, texture_rbga_stride, texture_tiles,
-                                 (size_t)0, (float *)nullptr);
+            launch_chained(true, grid, tp::kTexThreads, tp::kTexSmemBytes, s, tex, gd, (const int *)woi, src, 0LL,
+                           (const int *)base, (const int *)num_texture_tiles, parity << 1, quarter, -quarter,
+                           port_offsets, p, texture_rbga_stride, texture_tiles, (size_t)0, (float *)nullptr);
         if (err != cudaSuccess) return cuda_status(err, "generate_RBGA texture pass launch");
     }
     return cuda_status(cudaGetLastError(), "generate_RBGA launch");
@@ -1240,7 +1239,7 @@ int tp_textures_accumulate_tc(const tp_geometry *g, const int *woi, float *const
     if ((rc = sm_count(&sms))) return rc;
     if ((rc = texture_smem_setup())) return rc;
     unsigned grid = grid_for((long long)num_texture_tiles, 1, sms, shape_per_sm(TP_SHAPE_TEXTURES));
-    tp::k_textures<true, true><<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
+    tex_kernel<true, true>(colors)<<<grid, tp::kTexThreads, tp::kTexSmemBytes, (cudaStream_t)stream>>>(
         gd, woi, tile_scratch, (long long)num_texture_tiles, texture_indices, nullptr, 0, 0, 0, port_offsets, p,
         want_rbg ? texture_rbg_stride : 0, want_rbg ? texture_rbg : nullptr, want_tiles ? texture_stride : 0,
         want_tiles ? texture_tiles : nullptr);

@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kFrameThreads, kFrameBlocksPerSm) k_frame(
             {
                 const int color = grp % 3;
                 float *cj = s_clt + grp * kJob, *xj = s_x + grp * kTB4;
-                imclt_unfold_job(cj, d_lpf[color], xj, nullptr, cj, l, gm);
+                imclt_unfold_job<false>(cj, d_lpf[color], xj, cj, l, gm);
                 debayer_job<false>(cj, xj, color < 2, p.tex.min_shot, p.tex.scale_shot, l, gm);
             }
             __syncthreads();

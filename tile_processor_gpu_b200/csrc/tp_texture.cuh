@@ -68,13 +68,15 @@ __device__ float d_tex_wi[256] = TP_TEX_WI_INIT;
  * writes those two columns whole, the quadrant signs of idct_signs
  * (:399-420) factored into a horizontal sign pair per column (per lane) and
  * a vertical sign per row (compile-time); the window factors are a per-lane
- * column factor times a compile-time row factor.  The first column a lane
+ * column factor, carried by the horizontal sign pair, times a compile-time
+ * row factor.  MONO: M (mono) instead of T (colour).  The first column a lane
  * writes is 11 - l: with job buffers 280 floats apart the four groups of a
  * warp then store to 32 distinct banks in both columns.  src: the job's
  * 4x64 coefficients (row stride 8), shared or global memory; tb: the
- * group's transpose buffer.  Either of mout and tout may be NULL. */
-__device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *mout,
-                                                 float *tout, int l, unsigned gm)
+ * group's transpose buffer; out: the job's [16][17] output tile. */
+template <bool MONO>
+__device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *out, int l,
+                                                 unsigned gm)
 {
     constexpr float kHwin[16] = TP_HWIN_INIT;
     float a[4][8]; /* pixel-domain column l of each quadrant */
@@ -109,9 +111,10 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
          * (-,+); 12-15: (-,-) on the (even, odd) quadrant of each pair) */
         const int c = h ? ((l < 4) ? l + 12 : l - 4) : 11 - l;
         const int cq = c >> 2;
-        const float s0 = (cq == 0) ? 1.0f : -1.0f, s1 = (cq == 3) ? -1.0f : 1.0f;
         const float wc = __ldg(&d_hwin[c]);
-        const float tcol = 0.25f / wc, mcol = 0.5f * wc;
+        /* the column's window factor: 0.5 w[c] (M) or 0.25 / w[c] (T) */
+        const float cf = MONO ? 0.5f * wc : 0.25f / wc;
+        const float s0 = (cq == 0) ? cf : -cf, s1 = (cq == 3) ? -cf : cf;
         float e0[8], e1[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
@@ -124,8 +127,7 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
             const int rq = r >> 2;
             /* vertical signs: rows 0-3 (+,+); 4-11 (-,+); 12-15 (-,-) */
             const float d = ((rq != 0) ? -e0[u] : e0[u]) + ((rq == 3) ? -e1[u] : e1[u]);
-            if (mout) mout[JT(r, c)] = (d * mcol) * (0.5f * kHwin[r]);
-            if (tout) tout[JT(r, c)] = (d * tcol) * (1.0f / kHwin[r]);
+            out[JT(r, c)] = d * (MONO ? 0.5f * kHwin[r] : 1.0f / kHwin[r]);
         }
     }
 }
@@ -382,8 +384,11 @@ constexpr size_t kTexSmemBytes = sizeof(float) * kTexSmemFloats;
 /* FROM_T: `clt` holds the jobs' pixel tiles instead of their CLT, as
  * k_tc_stage<InvTcStage> writes them (the un-windowed T for colour, the
  * windowed M for mono, [16][16] row-major at the job's CLT offset): stage 1
- * copies the tile into shared memory instead of inverting the CLT. */
-template <bool FROM_T, bool ALL>
+ * copies the tile into shared memory instead of inverting the CLT.
+ * ALL: the texture-tile outputs and the keep-weights statistics are built
+ * (false: the RGBA image only).  COLORS: the colour count, 1 or 3 (p.colors;
+ * a compile-time count lets each form keep only its own colour path). */
+template <bool FROM_T, bool ALL, int COLORS>
 __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     Geom g, const int *__restrict__ woi, float *const *clt, long long num_texture_tiles,
     const int *__restrict__ list, const int *__restrict__ dev_counts, int count_slot, int list_cap,
@@ -400,7 +405,8 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     const int tid = threadIdx.x;
     const int l = tid & 7, grp = tid >> 3;
     const unsigned gm = group_mask();
-    const int colors = p.colors;
+    static_assert(COLORS == 1 || COLORS == 3, "colour count");
+    constexpr int colors = COLORS;
     const int njobs = 4 * colors;
     /* 1 / (2 sigma^2) times log2(e): the fusion's weights are powers of two */
     const float ksigma = (float)(1.0 / (2.0 * (double)p.diff_sigma * (double)p.diff_sigma)) * kLog2e;
@@ -416,7 +422,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
         s_chw[0] = p.w0; s_chw[1] = p.w1; s_chw[2] = p.w2;
         /* the RGBA-only colour path debayers without the window (see
          * debayer_job): its distance factors carry the shot scale */
-        const float dsc = (!ALL && p.colors == 3 && p.scale_shot > 0.0f) ? p.scale_shot : 1.0f;
+        const float dsc = (!ALL && COLORS == 3 && p.scale_shot > 0.0f) ? p.scale_shot : 1.0f;
         for (int c = 0; c < 3; c++) s_chws[c] = sqrtf(s_chw[c]) * dsc;
     }
     /* D tiles come with the window and the shot scale in the ALL form and
@@ -556,11 +562,10 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
             if (colors > 1) {
                 /* T -> s_t, then the debayered D -> s_x (the transpose
                  * buffer, free once the unfold has read it) */
-                imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[color], xj, nullptr, tj, l,
-                                 gm);
+                imclt_unfold_job<false>(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[color], xj, tj, l, gm);
                 debayer_job<ALL>(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
             } else {
-                imclt_unfold_job(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[3], xj, tj, nullptr, l, gm);
+                imclt_unfold_job<true>(s_cp[cam] + ((size_t)tile * 3 + color) * 256, d_lpf[3], xj, tj, l, gm);
             }
         }
         __syncthreads();
