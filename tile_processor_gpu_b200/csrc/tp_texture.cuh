@@ -5,8 +5,8 @@
  * :4202-4665).
  *
  * One 96-thread block (three warps) per listed tile (grid-stride), seven
- * blocks per SM (80 registers, 27 KB of shared memory each: the tiles T and
- * D only).  The CLT is read straight from global memory by the inverse
+ * blocks per SM (at most 80 registers, 27 KB of shared memory each: the
+ * tiles T and D only).  The CLT is read straight from global memory by the inverse
  * transform; the next tile's CLT and the RGBA rows it will update are
  * prefetched into L2 while the block works on the current tile.  Per
  * (camera, color) job one 8-lane group, working only with __syncwarp on its
