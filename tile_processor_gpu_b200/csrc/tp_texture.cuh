@@ -163,16 +163,16 @@ __device__ __forceinline__ float rcp_hw(float x)
  * WINDOWED = false stores D
  * without them (the camera fusion of the RGBA-only path measures distances
  * in D wi sqrt(w) scale_shot, where the squared window cancels against wi =
- * 1 / wnd2: it takes scale_shot with its colour factors instead). */
-template <bool WINDOWED>
-__device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mode, float min_shot,
-                                            float scale_shot, int l, unsigned gm)
+ * 1 / wnd2: it takes scale_shot with its colour factors instead).  SHOT:
+ * scale_shot > 0, the shot-noise step applies. */
+template <bool WINDOWED, bool SHOT>
+__device__ __forceinline__ void debayer_tile(const float *t, float *d, int rb_mode, float min_shot,
+                                             float scale_shot, int l, unsigned gm)
 {
     /* the window as compile-time constants (the values of c_hwin): the
      * squared window of an unrolled row folds into an immediate operand */
     constexpr float kHwin[16] = TP_HWIN_INIT;
     __syncwarp(gm);
-    const bool shot = scale_shot > 0.0f;
     const float kdiag = rb_mode ? 0.0625f : 0.0f, kcenter = rb_mode ? 0.25f : 0.5f;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -182,7 +182,7 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
         /* per-lane stencil weights: diagonal, orthogonal, centre */
         const float kd = cborder ? 0.0f : kdiag, ko = cborder ? 0.0f : 0.125f, kc = cborder ? 1.0f : kcenter;
         const float hcc = __ldg(&d_hwin[c]);
-        const float swx = (shot ? scale_shot : 1.0f) * (hcc * hcc);
+        const float swx = (SHOT ? scale_shot : 1.0f) * (hcc * hcc);
         float a1 = t[JT(0, c)], ha = t[JT(0, cm)] + t[JT(0, cp)];
         float b1 = t[JT(1, c)], hb = t[JT(1, cm)] + t[JT(1, cp)];
 #pragma unroll
@@ -204,11 +204,23 @@ __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mod
              * below it: both are v * rsqrt(max(v, min_shot)) (min_shot is a
              * normal float > 0 whenever the transform applies), from the
              * hardware reciprocal square root (within 3e-7 of sqrtf) */
-            if (shot) v = v * rsqrt_hw(fmaxf(v, min_shot));
+            if (SHOT) v = v * rsqrt_hw(fmaxf(v, min_shot));
             d[JT(r, c)] = WINDOWED ? v * (swx * (kHwin[r] * kHwin[r])) : v;
         }
     }
     __syncwarp(gm);
+}
+
+/* debayer_tile with the shot-noise step compiled in (scale_shot > 0) or out:
+ * one switch per job, outside the unrolled stencil */
+template <bool WINDOWED>
+__device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mode, float min_shot,
+                                            float scale_shot, int l, unsigned gm)
+{
+    if (scale_shot > 0.0f)
+        debayer_tile<WINDOWED, true>(t, d, rb_mode, min_shot, scale_shot, l, gm);
+    else
+        debayer_tile<WINDOWED, false>(t, d, rb_mode, min_shot, scale_shot, l, gm);
 }
 
 /* log2(e): e^x = 2^(x log2 e) */
