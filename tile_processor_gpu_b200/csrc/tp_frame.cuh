@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kFrameThreads, kFrameBlocksPerSm) k_frame(
                     for (int sl = 0; sl < 4; sl++) old[sl] = b[(size_t)sl * slice_stride];
                 }
                 float o[12];
-                combine_pixel<3, false>(s_x, kTB4, s_clt, kJob, wnd2, JT(r, c), s_pd2r, ksigma, s_chw, s_chws, wnd2,
+                combine_pixel<3, false>(s_x, kTB4, s_clt, kJob, wnd2, JTS(kJS, r, c), s_pd2r, ksigma, s_chw, s_chws, wnd2,
                                         wi, p.tex.dust_remove, 0, o);
                 if (!b) continue;
                 const float f = (nbr != TP_TASK_TEXTURE_BITS) ? __ldg(&d_alpha_fade[nbr][px]) : 1.0f;

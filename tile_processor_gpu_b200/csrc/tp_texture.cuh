@@ -37,8 +37,17 @@ struct TextureParams {
     int dust_remove, keep_weights;
 };
 
-constexpr int kJob = 280;        /* floats per 16x17 job tile, padded */
-#define JT(r, c) ((r) * 17 + (c))
+constexpr int kJob = 280; /* floats per job tile (16 rows of at most 17), padded */
+/* Pixel (r, c) of a job tile with row stride S.  The camera fusion reads 32
+ * consecutive pixels (two rows) per warp: at stride 16 they fall on 32
+ * distinct banks, at 17 the second row's last pixel shares the first row's
+ * first bank.  The column-wise passes (unfold, debayer: one column per lane,
+ * the four groups' tiles 280 floats apart) are conflict-free at either
+ * stride.  Tiles copied in row by row (one row per lane, the tensor-core
+ * inverse's output) keep stride 17, where those stores spread over the
+ * banks. */
+#define JTS(S, r, c) ((r) * (S) + (c))
+constexpr int kJS = 16; /* row stride of tiles the inverse transform writes */
 
 __device__ __forceinline__ int sym8(int i) { return (i & 8) ? (i ^ 15) : i; }
 
@@ -56,7 +65,7 @@ __device__ float d_tex_wnd2[256] = TP_TEX_WND2_INIT;
 __device__ float d_tex_wi[256] = TP_TEX_WI_INIT;
 
 /* Windowed inverse CLT of one job (imclt8threads, :3847-4017) into the
- * [16][17] tile M = w * d (w the product of the two half-sine windows, no
+ * [16][kJS] tile M = w * d (w the product of the two half-sine windows, no
  * accumulation), and, for the debayer, the same tile with the squared window
  * removed, T = M / (sin^2 r sin^2 c) = d / (4 sin r sin c), formed directly
  * from the signed sum d.  Lane l loads coefficient row l of each quadrant (two
@@ -73,7 +82,7 @@ __device__ float d_tex_wi[256] = TP_TEX_WI_INIT;
  * writes is 11 - l: with job buffers 280 floats apart the four groups of a
  * warp then store to 32 distinct banks in both columns.  src: the job's
  * 4x64 coefficients (row stride 8), shared or global memory; tb: the
- * group's transpose buffer; out: the job's [16][17] output tile. */
+ * group's transpose buffer; out: the job's [16][kJS] output tile. */
 template <bool MONO>
 __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *lpf, float *tb, float *out, int l,
                                                  unsigned gm)
@@ -127,7 +136,7 @@ __device__ __forceinline__ void imclt_unfold_job(const float *src, const float *
             const int rq = r >> 2;
             /* vertical signs: rows 0-3 (+,+); 4-11 (-,+); 12-15 (-,-) */
             const float d = ((rq != 0) ? -e0[u] : e0[u]) + ((rq == 3) ? -e1[u] : e1[u]);
-            out[JT(r, c)] = d * (MONO ? 0.5f * kHwin[r] : 1.0f / kHwin[r]);
+            out[JTS(kJS, r, c)] = d * (MONO ? 0.5f * kHwin[r] : 1.0f / kHwin[r]);
         }
     }
 }
@@ -164,8 +173,8 @@ __device__ __forceinline__ float rcp_hw(float x)
  * without them (the camera fusion of the RGBA-only path measures distances
  * in D wi sqrt(w) scale_shot, where the squared window cancels against wi =
  * 1 / wnd2: it takes scale_shot with its colour factors instead).  SHOT:
- * scale_shot > 0, the shot-noise step applies. */
-template <bool WINDOWED, bool SHOT>
+ * scale_shot > 0, the shot-noise step applies.  S: the tiles' row stride. */
+template <bool WINDOWED, bool SHOT, int S>
 __device__ __forceinline__ void debayer_tile(const float *t, float *d, int rb_mode, float min_shot,
                                              float scale_shot, int l, unsigned gm)
 {
@@ -183,8 +192,8 @@ __device__ __forceinline__ void debayer_tile(const float *t, float *d, int rb_mo
         const float kd = cborder ? 0.0f : kdiag, ko = cborder ? 0.0f : 0.125f, kc = cborder ? 1.0f : kcenter;
         const float hcc = __ldg(&d_hwin[c]);
         const float swx = (SHOT ? scale_shot : 1.0f) * (hcc * hcc);
-        float a1 = t[JT(0, c)], ha = t[JT(0, cm)] + t[JT(0, cp)];
-        float b1 = t[JT(1, c)], hb = t[JT(1, cm)] + t[JT(1, cp)];
+        float a1 = t[JTS(S, 0, c)], ha = t[JTS(S, 0, cm)] + t[JTS(S, 0, cp)];
+        float b1 = t[JTS(S, 1, c)], hb = t[JTS(S, 1, cm)] + t[JTS(S, 1, cp)];
 #pragma unroll
         for (int r = 0; r < 16; r++) {
             float v;
@@ -193,7 +202,7 @@ __device__ __forceinline__ void debayer_tile(const float *t, float *d, int rb_mo
             } else if (r == 15) {
                 v = b1;
             } else {
-                const float e1 = t[JT(r + 1, c)], he = t[JT(r + 1, cm)] + t[JT(r + 1, cp)];
+                const float e1 = t[JTS(S, r + 1, c)], he = t[JTS(S, r + 1, cm)] + t[JTS(S, r + 1, cp)];
                 const float orth = (a1 + e1) + hb;
                 const float diag = ha + he;
                 v = __fmaf_rn(kd, diag, __fmaf_rn(ko, orth, kc * b1));
@@ -205,7 +214,7 @@ __device__ __forceinline__ void debayer_tile(const float *t, float *d, int rb_mo
              * normal float > 0 whenever the transform applies), from the
              * hardware reciprocal square root (within 3e-7 of sqrtf) */
             if (SHOT) v = v * rsqrt_hw(fmaxf(v, min_shot));
-            d[JT(r, c)] = WINDOWED ? v * (swx * (kHwin[r] * kHwin[r])) : v;
+            d[JTS(S, r, c)] = WINDOWED ? v * (swx * (kHwin[r] * kHwin[r])) : v;
         }
     }
     __syncwarp(gm);
@@ -213,14 +222,14 @@ __device__ __forceinline__ void debayer_tile(const float *t, float *d, int rb_mo
 
 /* debayer_tile with the shot-noise step compiled in (scale_shot > 0) or out:
  * one switch per job, outside the unrolled stencil */
-template <bool WINDOWED>
+template <bool WINDOWED, int S = kJS>
 __device__ __forceinline__ void debayer_job(const float *t, float *d, int rb_mode, float min_shot,
                                             float scale_shot, int l, unsigned gm)
 {
     if (scale_shot > 0.0f)
-        debayer_tile<WINDOWED, true>(t, d, rb_mode, min_shot, scale_shot, l, gm);
+        debayer_tile<WINDOWED, true, S>(t, d, rb_mode, min_shot, scale_shot, l, gm);
     else
-        debayer_tile<WINDOWED, false>(t, d, rb_mode, min_shot, scale_shot, l, gm);
+        debayer_tile<WINDOWED, false, S>(t, d, rb_mode, min_shot, scale_shot, l, gm);
 }
 
 /* log2(e): e^x = 2^(x log2 e) */
@@ -419,6 +428,9 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
     const unsigned gm = group_mask();
     static_assert(COLORS == 1 || COLORS == 3, "colour count");
     constexpr int colors = COLORS;
+    /* row stride of the T and D tiles: 17 where stage 1 copies T in row by
+     * row (FROM_T), else that of the inverse transform's output */
+    constexpr int kS = FROM_T ? 17 : kJS;
     const int njobs = 4 * colors;
     /* 1 / (2 sigma^2) times log2(e): the fusion's weights are powers of two */
     const float ksigma = (float)(1.0 / (2.0 * (double)p.diff_sigma * (double)p.diff_sigma)) * kLog2e;
@@ -565,9 +577,9 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
                 load_row8(src + 16 * h, al16, v);
                 load_row8(src + 16 * h + 8, al16, v + 8);
 #pragma unroll
-                for (int c = 0; c < 16; c++) tj[JT(2 * l + h, c)] = v[c];
+                for (int c = 0; c < 16; c++) tj[JTS(kS, 2 * l + h, c)] = v[c];
             }
-            if (colors > 1) debayer_job<ALL>(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
+            if (colors > 1) debayer_job<ALL, kS>(tj, xj, color < 2, p.min_shot, p.scale_shot, l, gm);
         } else if (grp < njobs) {
             const int cam = grp / colors, color = grp - cam * colors;
             float *tj = s_t + grp * kJob, *xj = s_x + grp * kTB4;
@@ -594,7 +606,7 @@ __global__ void __launch_bounds__(kTexThreads, 7) k_textures(
 #pragma unroll 1
         for (int px = tid; px < 256; px += kTexThreads) {
             const int r = px >> 4, c = px & 15;
-            const int e = JT(r, c);
+            const int e = JTS(kS, r, c);
             const float wnd2 = __ldg(&d_tex_wnd2[px]), wi = __ldg(&d_tex_wi[px]);
             /* the pixel's RGBA values are loaded before the fusion, whose
              * arithmetic then covers their latency */
