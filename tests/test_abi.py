@@ -86,6 +86,11 @@ def test_rejects_bad_arguments(native):
                                 .3, .1, .6, 1, 0, 0, None, 1024, fake, None)) == N.TP_ERR_ARG
     assert _code(lambda: N.call("tp_textures_accumulate", g.ptr, None, fake, 4, fake, fake, *args, 1, 0, None, 1024,
                                 fake, None)) == N.TP_ERR_ARG
+    # a colour count other than 1 or 3 (the texture kernels are built per
+    # count); the shot-noise step without a positive min_shot
+    for bad in ((2,) + args[1:], (3, 0, 0.0, 3.) + args[4:], (3, 0, -1.0, 3.) + args[4:]):
+        assert _code(lambda: N.call("tp_textures_accumulate", g.ptr, None, fake, 4, fake, fake, *bad, 0, 0, None, 1024,
+                                    fake, None)) == N.TP_ERR_ARG
     # RGBA output without a window of interest
     assert _code(lambda: N.call("tp_textures_accumulate", g.ptr, None, fake, 4, fake, fake, *args, 0, 300, fake, 0,
                                 None, None)) == N.TP_ERR_ARG
