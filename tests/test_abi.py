@@ -138,6 +138,25 @@ def test_launch_shapes(native):
         assert _code(lambda: N.call("tp_set_launch_shape", kernel, v)) == N.TP_ERR_ARG
     assert _code(lambda: N.call("tp_get_launch_shape", 7)) == N.TP_ERR_ARG
     assert A.get_shape("convert") == 8
+
+
+def test_tuner_keeps_the_fastest_cap(native, monkeypatch):
+    """autotune.tune times the workload under each candidate cap (here a fake
+    timer that reads the cap in force) and leaves the fastest one set."""
+    from tile_processor_gpu_b200 import autotune as A
+    fake_ms = {4: 0.41, 6: 0.43, 8: 0.39, 12: 0.385, 16: 0.40}
+    seen = []
+    monkeypatch.setattr(A, "time_ms", lambda run, repeats, warmup: (seen.append(A.get_shape("correlate")),
+                                                                     fake_ms[A.get_shape("correlate")])[1])
+    try:
+        best, times = A.tune("correlate", run=lambda: None)
+        assert best == 12 and A.get_shape("correlate") == 12
+        assert seen == list(A.CANDIDATES["correlate"]) and times == fake_ms
+        best, _ = A.tune("correlate", run=lambda: None, candidates=(16, 4))
+        assert best == 16 and A.get_shape("correlate") == 16
+    finally:
+        A.reset()
+    assert A.get_shape("correlate") == 8
     # the tuner never steps off the built-in shape: each default is a candidate
     for k in A.KERNELS:
         assert A.get_shape(k) in A.CANDIDATES[k]
