@@ -169,11 +169,11 @@ __device__ __forceinline__ float rcp_hw(float x)
  * hold different colours, do not diverge; the border columns (copied
  * unchanged) take the same form with stencil weights 0, 0 and 1.  The
  * shot-noise scale and the two window factors are one product per pixel.
- * WINDOWED = false stores D
- * without them (the camera fusion of the RGBA-only path measures distances
- * in D wi sqrt(w) scale_shot, where the squared window cancels against wi =
- * 1 / wnd2: it takes scale_shot with its colour factors instead).  SHOT:
- * scale_shot > 0, the shot-noise step applies.  S: the tiles' row stride. */
+ * WINDOWED = false stores D without them (the camera fusion of the RGBA-only
+ * path measures distances in D wi sqrt(w) scale_shot, where the squared
+ * window cancels against wi = 1 / wnd2: it takes scale_shot with its colour
+ * factors instead).  SHOT: scale_shot > 0, the shot-noise step applies.
+ * S: the tiles' row stride. */
 template <bool WINDOWED, bool SHOT, int S>
 __device__ __forceinline__ void debayer_tile(const float *t, float *d, int rb_mode, float min_shot,
                                              float scale_shot, int l, unsigned gm)
